@@ -1,0 +1,416 @@
+#!/usr/bin/env python
+"""Benchmark of the extrapolation + imaging path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload NAME]
+
+One step = one full migration (every shot x frequency x depth step, imaging included) of the
+workload with inputs resident in HBM.  The default workload is `batched_uneven`: nz=1000,
+nx=2048, nf=512 (2-50 Hz), 2M+1=35 taps, nk=4000, 256 shots with apertures U[256, 2048] (seeded
+synthetic data).  Metric: extrapolated points (shot, w, z, x) per second, whole job.
+
+Multi-GPU (torchrun, one rank per GPU): weak scaling; every rank migrates its own shot set of the
+same size and the stacked images are summed with one all-reduce per step.
+
+Prints one JSON line (rank 0).  Other modes:
+  --impl reference   the reference's own CPU library (oracle/_ref/extrapolation_cpu.so, all host
+                     threads) on a bounded sample of the same workload, same metric.
+"""
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
+
+import numpy as np  # noqa: E402
+
+METRIC = "extrapolated pts/s (shot*w*z*x), batched vs plain on 1 GPU; rel-L2 err vs FP64"
+UNIT = "pts/s"
+
+
+def parse_args():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--workload", default="batched_uneven")
+    p.add_argument("--scale", type=float, default=1.0)
+    p.add_argument("--e2e-steps", type=int, default=2)
+    p.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU-baseline sample time")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-naive", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--accuracy", action="store_true", help="also measure rel-L2 vs the FP64 oracle on a sub-volume")
+    return p.parse_args()
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi samples every 200 ms while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+
+        sm = [num(r[1]) for r in rows if num(r[1])]
+        mx = [num(r[2]) for r in rows if num(r[2])]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for i, n in enumerate(names):
+                if r[5 + i].lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+class quiet_stdout:
+    """Send file descriptor 1 to stderr while a C library that prints on stdout runs."""
+
+    def __enter__(self):
+        sys.stdout.flush()
+        self.saved = os.dup(1)
+        os.dup2(2, 1)
+
+    def __exit__(self, *exc):
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
+
+
+def reference_sample(w, target_s, max_table_bytes=1 << 30):
+    """Time the reference CPU library on a bounded sample of workload w: the first shots, all
+    frequencies, a leading depth slab; dense tables gathered from the compact table beforehand
+    (not timed, as the reference's EXTRAPOLATION/IMAGING timers exclude table building).
+    Returns (points, seconds, description)."""
+    from oracle import oracle
+    if not oracle.have_ref():
+        raise RuntimeError("oracle/_ref/extrapolation_cpu.so missing")
+    L = w.L
+
+    def run(s, depth):
+        x0, n = int(w.shot_x0[s]), int(w.shot_nx[s])
+        tf = oracle.gather_dense_slab(0, depth, w.nx, x0, n, w.nf, w.M, w.nk, w.dk, w.omega, w.velocity, w.table)
+        tb = oracle.gather_dense_slab(0, depth, w.nx, x0, n, w.nf, w.M, w.nk, w.dk, w.omega, w.velocity, w.table,
+                                      conj_rows=True)
+        wave = np.ascontiguousarray(w.block(w.wave, s)[None])
+        shot = np.ascontiguousarray(w.block(w.shot, s)[None])
+        img = np.zeros((1, depth, n), dtype=np.float32)
+        with quiet_stdout():  # the reference library prints its phase timers on stdout
+            t0 = time.perf_counter()
+            oracle.ref_extrapolate(1, depth, depth, n, w.nf, w.nf, w.M, tf, tb, wave, shot, img)
+            t1 = time.perf_counter()
+        return n * w.nf * depth, t1 - t0
+
+    # calibrate on a 2-step slab of shot 0
+    p0, t0 = run(0, 2)
+    rate = p0 / max(t0, 1e-6)
+    order = np.argsort(-w.shot_nx)  # widest first: representative, not cheapest
+    want = rate * target_s
+    pts = 0
+    secs = 0.0
+    used = []
+    for s in order:
+        n = int(w.shot_nx[s])
+        depth = int(min(w.nextrap, max(1, (want - pts) // (n * w.nf)),
+                        max(1, max_table_bytes // (w.nf * n * L * 8))))
+        p, t = run(int(s), depth)
+        pts += p
+        secs += t
+        used.append((int(s), depth))
+        if pts >= want:
+            break
+    desc = (f"reference extrapolation_cpu.so, {len(used)} shot(s) of the workload (widest first), all {w.nf} "
+            f"frequencies, leading depth slabs {[d for _, d in used]}, {pts:.3g} points; dense tables gathered "
+            "beforehand and not timed")
+    return pts, secs, desc
+
+
+def run_reference_impl(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from imaging2d_wlsq_b200 import synthetic
+    w = synthetic.WORKLOADS[args.workload](scale=args.scale)
+    rates = []
+    desc = ""
+    t_all = 0.0
+    for i in range(args.warmup + args.steps):
+        pts, secs, desc = reference_sample(w, max(2.0, args.cpu_seconds / 2))
+        if i >= args.warmup:
+            rates.append(pts / secs)
+            t_all += secs
+    value = float(np.median(rates))
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t_all / max(1, args.steps),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c64 (fp32)",
+        "data": "synthetic (seeded)", "config": workload_config(w, args),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference", "sample": desc},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def workload_config(w, args):
+    return {"workload": f"{w.name}: nz={w.nz} nx={w.nx} dx={w.dx} nf={w.nf} taps={w.L} nk={w.nk} ns={w.ns} "
+                        f"apertures {int(w.shot_nx.min())}-{int(w.shot_nx.max())} (mean {w.shot_nx.mean():.0f})",
+            "points_per_step": w.points(), "scale": args.scale, "seed": w.seed,
+            "l2": "inputs (wavefields %.2f GB) larger than L2 (126 MB); no flush" % (2 * w.wave.nbytes / 1e9)}
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        return run_reference_impl(args)
+
+    import torch
+    import torch.distributed as dist
+    from imaging2d_wlsq_b200 import migration, synthetic
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+
+    # weak scaling: each rank its own seeded shot set of the full per-GPU size
+    maker = synthetic.WORKLOADS[args.workload]
+    w = maker(seed=100 + rank, scale=args.scale) if world > 1 else maker(scale=args.scale)
+    plan = migration.Plan.for_workload(w)
+    om = torch.from_numpy(w.omega).to(dev)
+    vel = torch.from_numpy(np.ascontiguousarray(w.velocity)).to(dev)
+    tab = torch.from_numpy(w.table).to(dev)
+    plan.set_model(om, vel, w.dk, tab)
+    wave0 = torch.from_numpy(w.wave).to(dev)
+    shot0 = torch.from_numpy(w.shot).to(dev)
+    wave = torch.empty_like(wave0)
+    shot = torch.empty_like(shot0)
+    image = torch.zeros((w.nz, w.nx), dtype=torch.float32, device=dev)
+    pts_rank = w.points()
+
+    def step():
+        wave.copy_(wave0)
+        shot.copy_(shot0)
+        plan.execute(wave, shot, image)
+        if world > 1:
+            dist.all_reduce(image)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    kernel_ms = []
+    e0.record()
+    for _ in range(args.steps):
+        step()
+        kernel_ms.append(plan.kernel_ms())
+    e1.record()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+    elapsed = e0.elapsed_time(e1) / 1e3
+    t = torch.tensor([elapsed], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    elapsed = float(t.item())
+    total_pts = pts_rank * world
+    value = total_pts * args.steps / elapsed
+    k_s = float(np.mean(kernel_ms)) / 1e3
+    describe = plan.describe()
+
+    extra = {}
+    if rank == 0:
+        fp32 = migration.fp32_peak_tflops()
+        flops_pt = 16 * w.L + 4
+        bytes_pt = 8 * w.L
+        hbm, hbm_src = peaks()
+        ach = pts_rank * flops_pt / k_s / 1e12
+        roof = {"bound": "fp32", "achieved": ach, "peak": fp32, "unit": "TFLOP/s", "frac": ach / fp32,
+                "traffic": None, "kernel": describe["kernel"], "kernel_ms": k_s * 1e3,
+                "per_point": f"{flops_pt} flop (16L+4, L={w.L})",
+                "peak_source": "FP32 FMA probe kernel timed in this run (img2d_measure_fp32_peak); "
+                               "MEASURED_PEAKS.json has no FP32 CUDA-core peak"}
+        ach_b = pts_rank * bytes_pt / k_s / 1e9
+        roof_hbm = {"bound": "hbm", "achieved": ach_b, "peak": hbm, "unit": "GB/s", "frac": ach_b / hbm,
+                    "per_point": f"{bytes_pt} B (8L operator bytes, no cross-shot reuse credit)",
+                    "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({hbm_src})",
+                    "note": "operator rows are served from L2/L1 and reused across the shots of a CTA, "
+                            "so this algorithmic-bytes ratio exceeds 1; the FP32 roofline binds"}
+        extra["roofline"] = roof
+        extra["roofline_hbm"] = roof_hbm
+        extra["kernel_config"] = describe
+
+    # end to end through the host C entry point, pinned host buffers, copies inside the timed region
+    if rank == 0 and not args.no_e2e:
+        hw = torch.from_numpy(w.wave).pin_memory()
+        hs = torch.from_numpy(w.shot).pin_memory()
+        wave_h = hw.numpy()
+        shot_h = hs.numpy()
+        img_h = torch.zeros((w.nz, w.nx), dtype=torch.float32).pin_memory().numpy()
+        from imaging2d_wlsq_b200._lib import check, lib, ptr
+        x0 = np.ascontiguousarray(w.shot_x0, dtype=np.int32)
+        wn = np.ascontiguousarray(w.shot_nx, dtype=np.int32)
+        vel_h = np.ascontiguousarray(w.velocity)
+
+        def e2e_call():
+            wave_h[:] = w.wave
+            shot_h[:] = w.shot
+            ta = torch.cuda.Event(enable_timing=True)
+            tb = torch.cuda.Event(enable_timing=True)
+            ta.record(torch.cuda.default_stream())
+            check(lib().img2d_migrate_compact(w.ns, w.nextrap, w.nz, w.nx, w.nf, w.nt, w.M, w.nk, float(w.dk),
+                                              ptr(w.omega), ptr(vel_h), ptr(w.table), None, ptr(x0), ptr(wn),
+                                              ptr(wave_h), ptr(shot_h), ptr(img_h), None, 0))
+            tb.record(torch.cuda.default_stream())
+            tb.synchronize()
+            return ta.elapsed_time(tb) / 1e3
+
+        e2e_call()
+        secs = [e2e_call() for _ in range(max(1, args.e2e_steps))]
+        h2d = w.wave.nbytes + w.shot.nbytes + w.omega.nbytes + w.nextrap * w.nx * 8 + w.table.nbytes
+        d2h = w.wave.nbytes + w.shot.nbytes + w.nextrap * w.nx * 4
+        extra["e2e"] = {"value": pts_rank / float(np.median(secs)), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+                        "d2h_bytes_per_step": int(d2h), "api": "img2d_migrate_compact (host buffers)",
+                        "n_gpus": 1}
+
+    # naive one-launch-per-(shot, w, z) form on a sample of the same workload
+    if rank == 0 and not args.no_naive:
+        nf_s = min(w.nf, 4)
+        ns_s = 1
+        sub = synthetic.Workload(w.name, w.nz, w.nx, w.dx, w.dz, nf_s, w.M, w.nk, w.dk, w.omega[:nf_s], w.velocity,
+                                 w.table, w.shot_x0[:ns_s], w.shot_nx[:ns_s], w.shot_pos[:ns_s], nextrap=w.nextrap)
+        sub.wave = np.ascontiguousarray(w.block(w.wave, 0)[:nf_s]).reshape(-1)
+        sub.shot = np.ascontiguousarray(w.block(w.shot, 0)[:nf_s]).reshape(-1)
+        nplan = migration.Plan.for_workload(sub)
+        nplan.set_model(torch.from_numpy(sub.omega.copy()).to(dev), vel, w.dk, tab)
+        sw = torch.from_numpy(sub.wave).to(dev)
+        ss = torch.from_numpy(sub.shot).to(dev)
+        si = torch.zeros((w.nz, w.nx), dtype=torch.float32, device=dev)
+        nplan.execute_naive(sw, ss, si)
+        torch.cuda.synchronize()
+        a0 = torch.cuda.Event(enable_timing=True)
+        a1 = torch.cuda.Event(enable_timing=True)
+        a0.record()
+        nplan.execute_naive(sw, ss, si)
+        a1.record()
+        a1.synchronize()
+        nsec = a0.elapsed_time(a1) / 1e3
+        npts = sub.points()
+        extra["plain_naive"] = {"value": npts / nsec, "unit": UNIT, "launches": ns_s * nf_s * (w.nextrap + 1),
+                                "sample": f"1 shot x {nf_s} frequencies x {w.nextrap} depths, one launch per "
+                                          "(shot, w, z)", "batched_over_naive": value / world / (npts / nsec)}
+        nplan.close()
+
+    if rank == 0 and not args.no_cpu_baseline and world == 1:
+        try:
+            pts, secs, desc = reference_sample(w, args.cpu_seconds)
+            extra["cpu_baseline"] = {"value": pts / secs, "unit": UNIT,
+                                     "cores": int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1)),
+                                     "kind": "reference", "sample": desc}
+        except Exception as ex:  # reference library not shipped with this tree
+            extra["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
+                                     "sample": f"unavailable: {ex}"}
+
+    if rank == 0 and args.accuracy:
+        from oracle import oracle
+        sub_n = min(w.nextrap, 40)
+        sub = maker(scale=args.scale) if world == 1 else w
+        plan_a = migration.Plan(sub.ns, sub_n, sub.nz, sub.nx, sub.nf, sub.nt, sub.M, sub.nk, sub.shot_x0, sub.shot_nx)
+        plan_a.set_model(om, vel, sub.dk, tab)
+        wa = torch.from_numpy(sub.wave).to(dev)
+        sa = torch.from_numpy(sub.shot).to(dev)
+        ia = torch.zeros((sub.nz, sub.nx), dtype=torch.float32, device=dev)
+        plan_a.execute(wa, sa, ia)
+        torch.cuda.synchronize()
+        stack, _, _, _ = oracle.migrate_workload_f64(sub, nextrap=sub_n)
+        got = ia.cpu().numpy().astype(np.float64)
+        extra["accuracy"] = {"rel_l2": float(np.linalg.norm(got - stack) / np.linalg.norm(stack)),
+                             "max_abs_rel": float(np.abs(got - stack).max() / np.abs(stack).max()),
+                             "sub_volume": f"first {sub_n} depth steps, all shots and frequencies",
+                             "reference": "FP64 CPU oracle"}
+        plan_a.close()
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * elapsed / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "c64 (fp32 complex)", "data": "synthetic (seeded)",
+            "config": dict(workload_config(w, args), parallelism=f"shots x{world} (weak)"),
+            "clocks": clk, "gpu_launches": 2 * args.steps,
+        }
+        line.update(extra)
+        print(json.dumps(line), flush=True)
+    plan.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,716 @@
+// C ABI of the B200 extrapolation + imaging library: plans, kernel dispatch and the
+// reference-compatible entry points.  Declarations and contracts: include/imaging2d_wlsq_b200.h.
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "../../include/imaging2d_wlsq_b200.h"
+#include "wlsq_kernels.cuh"
+
+namespace img2d {
+
+static thread_local std::string g_err;
+
+static int fail(int code, const std::string &msg)
+{
+    g_err = msg;
+    return code;
+}
+
+#define IMG2D_CUDA(call)                                                                   \
+    do {                                                                                   \
+        cudaError_t e_ = (call);                                                           \
+        if (e_ != cudaSuccess) {                                                           \
+            cudaGetLastError();                                                            \
+            return fail(e_ == cudaErrorMemoryAllocation ? IMG2D_ENOMEM : IMG2D_ECUDA,      \
+                        std::string(#call) + ": " + cudaGetErrorString(e_));               \
+        }                                                                                  \
+    } while (0)
+
+typedef void (*KernelFn)(MigrateArgs);
+
+// ---------------------------------------------------------------------------------------
+// Kernel tables.  The fixed-length kernel is instantiated for the operator lengths of the
+// reference tests and of the benchmark configurations; any other length runs on the generic
+// kernel.
+// ---------------------------------------------------------------------------------------
+constexpr int kX = 8;
+
+template <int G, int L>
+struct FixedEntry {
+    static constexpr int g = G, l = L;
+};
+
+struct FixedKernel {
+    int G, L;
+    KernelFn fn;
+};
+
+#define IMG2D_FIXED(G, L) {G, L, migrate_fixed_kernel<G, kX, L, OP_CONJ>}
+#define IMG2D_FIXED_L(L) IMG2D_FIXED(1, L), IMG2D_FIXED(2, L), IMG2D_FIXED(4, L), IMG2D_FIXED(8, L)
+
+static const FixedKernel kFixed[] = {
+    IMG2D_FIXED_L(3),  IMG2D_FIXED_L(5),  IMG2D_FIXED_L(11), IMG2D_FIXED_L(25),
+    IMG2D_FIXED_L(31), IMG2D_FIXED_L(35), IMG2D_FIXED_L(43), IMG2D_FIXED_L(55),
+};
+
+static KernelFn find_fixed(int G, int L)
+{
+    for (const auto &k : kFixed)
+        if (k.G == G && k.L == L) return k.fn;
+    return nullptr;
+}
+
+static KernelFn find_generic(int G, int mode)
+{
+#define IMG2D_GEN(GG)                                                        \
+    if (G == GG) {                                                           \
+        if (mode == OP_CONJ) return migrate_generic_kernel<GG, OP_CONJ>;     \
+        if (mode == OP_TWO) return migrate_generic_kernel<GG, OP_TWO>;       \
+        return migrate_generic_kernel<GG, OP_DENSE>;                         \
+    }
+    IMG2D_GEN(1) IMG2D_GEN(2) IMG2D_GEN(4) IMG2D_GEN(8)
+#undef IMG2D_GEN
+    return nullptr;
+}
+
+// ---------------------------------------------------------------------------------------
+// Naive comparison kernel: one launch per (shot, frequency, depth), one thread per position,
+// wavefields and operators in global memory.
+// ---------------------------------------------------------------------------------------
+__global__ void naive_step_kernel(const float4 *__restrict__ cur, float4 *__restrict__ nxt, int w,
+                                  int M, const cpx *__restrict__ tab, int tab_stride,
+                                  const uint16_t *__restrict__ idx_row, int x0,
+                                  float *__restrict__ image_row)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= w) return;
+    const cpx *t = tab + (long long)idx_row[x0 + i] * tab_stride;
+    float sr = 0.f, si = 0.f, rr = 0.f, ri = 0.f;
+    for (int k = 0; k <= 2 * M; ++k) {
+        const float4 v = cur[i + k];
+        const cpx f = t[k];
+        sr = fmaf(f.re, v.x, sr); sr = fmaf(-f.im, v.y, sr);
+        si = fmaf(f.re, v.y, si); si = fmaf(f.im, v.x, si);
+        rr = fmaf(f.re, v.z, rr); rr = fmaf(-f.im, v.w, rr);
+        ri = fmaf(f.re, v.w, ri); ri = fmaf(f.im, v.z, ri);
+    }
+    nxt[i + M] = make_float4(sr, si, rr, ri);
+    atomicAdd(image_row + x0 + i, sr * rr - si * ri);
+}
+
+__global__ void naive_pack_kernel(const cpx *__restrict__ wave, const cpx *__restrict__ shot, int w,
+                                  int M, float4 *__restrict__ buf, int to_buf)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= w) return;
+    if (to_buf) {
+        const cpx S = wave[i], R = shot[i];
+        buf[i + M] = make_float4(S.re, S.im, R.re, -R.im);
+    }
+}
+
+__global__ void naive_unpack_kernel(const float4 *__restrict__ buf, int w, int M,
+                                    cpx *__restrict__ wave, cpx *__restrict__ shot)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= w) return;
+    const float4 v = buf[i + M];
+    wave[i] = cpx{v.x, v.y};
+    shot[i] = cpx{v.z, -v.w};
+}
+
+// FP32 FMA probe: 16 independent chains per thread so the FMA pipe, not latency, limits it.
+__global__ void fma_probe_kernel(float *out, int iters)
+{
+    float a[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) a[i] = threadIdx.x * 1e-3f + i;
+    const float b = 0.9999f, c = 1e-4f;
+    for (int it = 0; it < iters; ++it) {
+#pragma unroll
+        for (int r = 0; r < 8; ++r)
+#pragma unroll
+            for (int i = 0; i < 16; ++i) a[i] = fmaf(a[i], b, c);
+    }
+    float s = 0.f;
+#pragma unroll
+    for (int i = 0; i < 16; ++i) s += a[i];
+    out[blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+
+// ---------------------------------------------------------------------------------------
+// Plan
+// ---------------------------------------------------------------------------------------
+struct DevBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+    ~DevBuf() { release(); }
+    void release()
+    {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    int ensure(size_t n)
+    {
+        if (n <= bytes && p) return IMG2D_OK;
+        release();
+        if (n == 0) n = 16;
+        cudaError_t e = cudaMalloc(&p, n);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            p = nullptr;
+            return fail(IMG2D_ENOMEM, "cudaMalloc(" + std::to_string(n) + " bytes): " + cudaGetErrorString(e));
+        }
+        bytes = n;
+        return IMG2D_OK;
+    }
+    template <class T> T *as() const { return static_cast<T *>(p); }
+};
+
+}  // namespace img2d
+
+struct img2d_plan {
+    int ns = 0, nextrap = 0, nz = 0, nx = 0, nf = 0, nt = 0, M = 0, L = 0, nk = 0, flags = 0;
+    int mode = img2d::OP_CONJ;
+    int G = 1, grid = 0, n_items = 0, max_w = 0, tab_stride = 0, idx_lstride = 0;
+    bool fixed = false;
+    img2d::KernelFn fn = nullptr;
+    size_t smem = 0;
+    std::vector<int> x0, w;
+    std::vector<long long> off;
+    long long wave_elems = 0;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    bool ev_recorded = false;
+    ~img2d_plan()
+    {
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+    }
+    img2d::DevBuf items, groups, group_shots, shot_win, shot_off, idx, tabF, tabB, partial, comp,
+        counter, naive_buf;
+    // dense tables (drop-in ABI) are owned by the caller of run_dense
+};
+
+namespace img2d {
+
+static int check_device()
+{
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n == 0) {
+        cudaGetLastError();
+        return fail(IMG2D_ENODEV, "no CUDA device visible to imaging2d_wlsq_b200");
+    }
+    return IMG2D_OK;
+}
+
+// Shared memory bytes of one CTA for groups of G shots over a union window of width W.
+static size_t smem_bytes(int G, int W, int M, int X)
+{
+    const int Mp = ((M + X - 1) / X) * X;
+    const int Wp = ((W + X - 1) / X) * X;
+    const int npos = Mp + Wp + Mp;
+    const size_t nslot = (size_t)npos / X * (X + 1);
+    return 2 * nslot * G * sizeof(float4);
+}
+
+static int build_plan(img2d_plan *p, int ns, int nextrap, int nz, int nx, int nf, int nt, int M,
+                      int nk, const int *shot_x0, const int *shot_nx, int flags, int mode)
+{
+    if (ns <= 0 || nextrap <= 0 || nz < nextrap || nx <= 0 || nf <= 0 || nt < nf || M < 0)
+        return fail(IMG2D_EINVAL, "invalid dimensions (need ns>0, 0<nextrap<=nz, nx>0, 0<nf<=nt, M>=0)");
+    if (mode != OP_DENSE && (nk <= 0 || nk > 65535))
+        return fail(IMG2D_EINVAL, "nk must be in [1, 65535]");
+    if ((long long)nf * nextrap * nx > (1ll << 40)) return fail(IMG2D_EINVAL, "problem too large");
+    p->ns = ns; p->nextrap = nextrap; p->nz = nz; p->nx = nx; p->nf = nf; p->nt = nt; p->M = M;
+    p->L = 2 * M + 1; p->nk = nk; p->flags = flags; p->mode = mode;
+    p->x0.assign(ns, 0);
+    p->w.assign(ns, nx);
+    for (int s = 0; s < ns; ++s) {
+        if (shot_x0) p->x0[s] = shot_x0[s];
+        if (shot_nx) p->w[s] = shot_nx[s];
+        if (p->x0[s] < 0 || p->w[s] <= 0 || p->x0[s] + p->w[s] > nx)
+            return fail(IMG2D_EINVAL, "shot " + std::to_string(s) + " aperture outside [0, nx)");
+    }
+    p->off.assign(ns, 0);
+    long long acc = 0;
+    for (int s = 0; s < ns; ++s) {
+        p->off[s] = acc;
+        acc += (long long)nt * p->w[s];
+    }
+    p->wave_elems = acc;
+
+    // Choose shots per CTA: the largest power of two <= 8 whose ping-pong buffers fit in shared
+    // memory for the widest aperture, not above the shot count rounded up to a power of two.
+    int dev = 0;
+    IMG2D_CUDA(cudaGetDevice(&dev));
+    int smem_optin = 0, nsm = 0;
+    IMG2D_CUDA(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    IMG2D_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    const int maxw = *std::max_element(p->w.begin(), p->w.end());
+    int nsp2 = 1;
+    while (nsp2 < ns) nsp2 <<= 1;
+    const int static_reserve = 1024;
+    int G = 8;
+    while (G > 1 && (G > nsp2 || smem_bytes(G, nx, M, kX) + static_reserve > (size_t)smem_optin)) G >>= 1;
+    const bool use_fixed = (mode == OP_CONJ) && !(flags & IMG2D_FLAG_GENERIC) && find_fixed(G, p->L);
+    const int X = use_fixed ? kX : 4;
+    if (smem_bytes(G, nx, M, X) + static_reserve > (size_t)smem_optin)
+        return fail(IMG2D_EINVAL, "aperture too wide for one CTA's shared memory");
+    p->G = G;
+    p->fixed = use_fixed;
+    p->fn = use_fixed ? find_fixed(G, p->L) : find_generic(G, mode);
+
+    // Group shots of similar aperture: sort by (x0, x1) and take consecutive runs of G.
+    std::vector<int> order(ns);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+        if (p->x0[a] != p->x0[b]) return p->x0[a] < p->x0[b];
+        return p->x0[a] + p->w[a] < p->x0[b] + p->w[b];
+    });
+    std::vector<int4> groups;
+    std::vector<int> gshots;
+    int widest = 0;
+    for (int g0 = 0; g0 < ns; g0 += G) {
+        int n = std::min(G, ns - g0), u0 = nx, u1 = 0;
+        for (int k = 0; k < n; ++k) {
+            int s = order[g0 + k];
+            u0 = std::min(u0, p->x0[s]);
+            u1 = std::max(u1, p->x0[s] + p->w[s]);
+            gshots.push_back(s);
+        }
+        groups.push_back(make_int4(g0, n, u0, u1 - u0));
+        widest = std::max(widest, u1 - u0);
+    }
+    p->max_w = widest;
+    p->smem = smem_bytes(G, widest, M, X);
+    // Items (group, frequency), widest groups first so the tail of the queue is short work.
+    std::vector<int2> items;
+    items.reserve(groups.size() * (size_t)nf);
+    std::vector<int> gorder(groups.size());
+    std::iota(gorder.begin(), gorder.end(), 0);
+    std::stable_sort(gorder.begin(), gorder.end(), [&](int a, int b) { return groups[a].w > groups[b].w; });
+    for (int g : gorder)
+        for (int j = 0; j < nf; ++j) items.push_back(make_int2(g, j));
+    p->n_items = (int)items.size();
+    p->grid = std::min(p->n_items, nsm);
+
+    std::vector<int2> win(ns);
+    for (int s = 0; s < ns; ++s) win[s] = make_int2(p->x0[s], p->w[s]);
+    int rc;
+    if ((rc = p->items.ensure(items.size() * sizeof(int2)))) return rc;
+    if ((rc = p->groups.ensure(groups.size() * sizeof(int4)))) return rc;
+    if ((rc = p->group_shots.ensure(gshots.size() * sizeof(int)))) return rc;
+    if ((rc = p->shot_win.ensure(win.size() * sizeof(int2)))) return rc;
+    if ((rc = p->shot_off.ensure(p->off.size() * sizeof(long long)))) return rc;
+    if ((rc = p->counter.ensure(sizeof(int)))) return rc;
+    IMG2D_CUDA(cudaMemcpy(p->items.p, items.data(), items.size() * sizeof(int2), cudaMemcpyHostToDevice));
+    IMG2D_CUDA(cudaMemcpy(p->groups.p, groups.data(), groups.size() * sizeof(int4), cudaMemcpyHostToDevice));
+    IMG2D_CUDA(cudaMemcpy(p->group_shots.p, gshots.data(), gshots.size() * sizeof(int), cudaMemcpyHostToDevice));
+    IMG2D_CUDA(cudaMemcpy(p->shot_win.p, win.data(), win.size() * sizeof(int2), cudaMemcpyHostToDevice));
+    IMG2D_CUDA(cudaMemcpy(p->shot_off.p, p->off.data(), p->off.size() * sizeof(long long), cudaMemcpyHostToDevice));
+    IMG2D_CUDA(cudaFuncSetAttribute(p->fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->smem));
+    const size_t plane = (size_t)nextrap * nx;
+    if ((rc = p->partial.ensure((size_t)p->grid * plane * sizeof(float)))) return rc;
+    if ((rc = p->comp.ensure((size_t)p->grid * plane * sizeof(float)))) return rc;
+    if (mode != OP_DENSE) {
+        p->idx_lstride = (nx + 7) / 8 * 8;
+        if ((rc = p->idx.ensure((size_t)nf * nextrap * p->idx_lstride * sizeof(uint16_t)))) return rc;
+        p->tab_stride = (p->L + 1) / 2 * 2;
+        if ((rc = p->tabF.ensure((size_t)nk * p->tab_stride * sizeof(cpx)))) return rc;
+        if (mode == OP_TWO && (rc = p->tabB.ensure((size_t)nk * p->tab_stride * sizeof(cpx)))) return rc;
+    }
+    return IMG2D_OK;
+}
+
+static MigrateArgs base_args(img2d_plan *p, cpx *wave, cpx *shot)
+{
+    MigrateArgs a{};
+    a.nextrap = p->nextrap;
+    a.nx = p->nx;
+    a.nf = p->nf;
+    a.M = p->M;
+    a.tab_stride = p->tab_stride;
+    a.n_items = p->n_items;
+    a.items = p->items.as<int2>();
+    a.groups = p->groups.as<int4>();
+    a.group_shots = p->group_shots.as<int>();
+    a.shot_win = p->shot_win.as<int2>();
+    a.shot_off = p->shot_off.as<long long>();
+    a.tabF = p->tabF.as<cpx>();
+    a.tabB = p->mode == OP_TWO ? p->tabB.as<cpx>() : p->tabF.as<cpx>();
+    a.idx = p->idx.as<uint16_t>();
+    a.idx_jstride = (long long)p->nextrap * p->idx_lstride;
+    a.idx_lstride = p->idx_lstride;
+    a.wave = wave;
+    a.shot = shot;
+    a.write_back = 1;
+    a.counter = p->counter.as<int>();
+    return a;
+}
+
+// Launch the persistent kernel and (optionally) reduce the stacked image.
+static int launch(img2d_plan *p, MigrateArgs a, float *d_image, float *d_image_shots,
+                  long long img_sstride, cudaStream_t st)
+{
+    const size_t plane = (size_t)p->nextrap * p->nx;
+    IMG2D_CUDA(cudaMemsetAsync(p->counter.p, 0, sizeof(int), st));
+    if (d_image) {
+        IMG2D_CUDA(cudaMemsetAsync(p->partial.p, 0, (size_t)p->grid * plane * sizeof(float), st));
+        IMG2D_CUDA(cudaMemsetAsync(p->comp.p, 0, (size_t)p->grid * plane * sizeof(float), st));
+        a.partial = p->partial.as<float>();
+        a.comp = p->comp.as<float>();
+    }
+    if (d_image_shots) {
+        IMG2D_CUDA(cudaMemset2DAsync(d_image_shots, img_sstride * sizeof(float), 0, plane * sizeof(float),
+                                     p->ns, st));
+        a.image_shots = d_image_shots;
+        a.img_sstride = img_sstride;
+    }
+    if (!p->ev0) {
+        IMG2D_CUDA(cudaEventCreate(&p->ev0));
+        IMG2D_CUDA(cudaEventCreate(&p->ev1));
+    }
+    IMG2D_CUDA(cudaEventRecord(p->ev0, st));
+    p->fn<<<p->grid, 256, p->smem, st>>>(a);
+    IMG2D_CUDA(cudaGetLastError());
+    IMG2D_CUDA(cudaEventRecord(p->ev1, st));
+    p->ev_recorded = true;
+    if (d_image) {
+        const int blocks = (int)std::min<size_t>((plane + 255) / 256, 148 * 8);
+        reduce_partials_kernel<<<blocks, 256, 0, st>>>(p->partial.as<float>(), p->comp.as<float>(), p->grid,
+                                                       (long long)plane, d_image);
+        IMG2D_CUDA(cudaGetLastError());
+    }
+    return IMG2D_OK;
+}
+
+static int set_model(img2d_plan *p, const double *d_omega, const double *d_vel, double dk,
+                     const cpx *d_tabF, const cpx *d_tabB, cudaStream_t st)
+{
+    if (!d_omega || !d_vel || !d_tabF || !(dk > 0.0))
+        return fail(IMG2D_EINVAL, "set_model needs omega, velocity, tab_forw and dk > 0");
+    if (p->mode == OP_TWO && !d_tabB) return fail(IMG2D_EINVAL, "two-table mode needs tab_back");
+    const size_t row = (size_t)p->L * sizeof(cpx), prow = (size_t)p->tab_stride * sizeof(cpx);
+    IMG2D_CUDA(cudaMemsetAsync(p->tabF.p, 0, (size_t)p->nk * prow, st));
+    IMG2D_CUDA(cudaMemcpy2DAsync(p->tabF.p, prow, d_tabF, row, row, p->nk, cudaMemcpyDeviceToDevice, st));
+    if (p->mode == OP_TWO) {
+        IMG2D_CUDA(cudaMemsetAsync(p->tabB.p, 0, (size_t)p->nk * prow, st));
+        IMG2D_CUDA(cudaMemcpy2DAsync(p->tabB.p, prow, d_tabB, row, row, p->nk, cudaMemcpyDeviceToDevice, st));
+    }
+    const long long total = (long long)p->nf * p->nextrap * p->nx;
+    const int blocks = (int)std::min<long long>((total + 255) / 256, 148 * 16);
+    index_table_kernel<<<blocks, 256, 0, st>>>(d_omega, d_vel, p->nf, p->nextrap, p->nx, p->idx_lstride, p->nk,
+                                               dk, p->idx.as<uint16_t>());
+    IMG2D_CUDA(cudaGetLastError());
+    return IMG2D_OK;
+}
+
+// Scoped device allocation for the host entry points.
+struct Scratch {
+    std::vector<void *> ptrs;
+    ~Scratch()
+    {
+        for (void *q : ptrs) cudaFree(q);
+    }
+    template <class T> int alloc(T **out, size_t n)
+    {
+        void *q = nullptr;
+        cudaError_t e = cudaMalloc(&q, n ? n : 16);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return fail(IMG2D_ENOMEM, "cudaMalloc(" + std::to_string(n) + " bytes): " + cudaGetErrorString(e));
+        }
+        ptrs.push_back(q);
+        *out = static_cast<T *>(q);
+        return IMG2D_OK;
+    }
+};
+
+// Dense-table drop-in: both argument orders come here.
+static int run_dense(int ns, int nextrap, int nz, int nx, int nf, int nt, int M, const cpx *opF,
+                     const cpx *opB, cpx *wave, cpx *shot, float *image, int write_back)
+{
+    int rc;
+    if ((rc = check_device())) return rc;
+    if (!opF || !opB || !wave || !shot || !image) return fail(IMG2D_EINVAL, "null pointer argument");
+    img2d_plan plan;
+    if ((rc = build_plan(&plan, ns, nextrap, nz, nx, nf, nt, M, 1, nullptr, nullptr, 0, OP_DENSE))) return rc;
+    Scratch sc;
+    const size_t L = 2 * (size_t)M + 1;
+    const size_t tab = (size_t)nextrap * nf * nx * L;
+    const size_t wel = (size_t)ns * nt * nx;
+    const size_t plane = (size_t)nz * nx;
+    cpx *dF, *dB, *dW, *dS;
+    float *dI;
+    if ((rc = sc.alloc(&dF, tab * sizeof(cpx)))) return rc;
+    if ((rc = sc.alloc(&dB, tab * sizeof(cpx)))) return rc;
+    if ((rc = sc.alloc(&dW, wel * sizeof(cpx)))) return rc;
+    if ((rc = sc.alloc(&dS, wel * sizeof(cpx)))) return rc;
+    if ((rc = sc.alloc(&dI, (size_t)ns * plane * sizeof(float)))) return rc;
+    IMG2D_CUDA(cudaMemcpy(dF, opF, tab * sizeof(cpx), cudaMemcpyHostToDevice));
+    IMG2D_CUDA(cudaMemcpy(dB, opB, tab * sizeof(cpx), cudaMemcpyHostToDevice));
+    IMG2D_CUDA(cudaMemcpy(dW, wave, wel * sizeof(cpx), cudaMemcpyHostToDevice));
+    IMG2D_CUDA(cudaMemcpy(dS, shot, wel * sizeof(cpx), cudaMemcpyHostToDevice));
+    MigrateArgs a = base_args(&plan, dW, dS);
+    a.denseF = dF;
+    a.denseB = dB;
+    if ((rc = launch(&plan, a, nullptr, dI, (long long)plane, 0))) return rc;
+    IMG2D_CUDA(cudaDeviceSynchronize());
+    // rows [0, nextrap) of every shot image
+    IMG2D_CUDA(cudaMemcpy2D(image, plane * sizeof(float), dI, plane * sizeof(float),
+                            (size_t)nextrap * nx * sizeof(float), ns, cudaMemcpyDeviceToHost));
+    if (write_back) {
+        // only the first nf rows of every (nt, nx) shot block carry data
+        IMG2D_CUDA(cudaMemcpy2D(wave, (size_t)nt * nx * sizeof(cpx), dW, (size_t)nt * nx * sizeof(cpx),
+                                (size_t)nf * nx * sizeof(cpx), ns, cudaMemcpyDeviceToHost));
+        IMG2D_CUDA(cudaMemcpy2D(shot, (size_t)nt * nx * sizeof(cpx), dS, (size_t)nt * nx * sizeof(cpx),
+                                (size_t)nf * nx * sizeof(cpx), ns, cudaMemcpyDeviceToHost));
+    }
+    return IMG2D_OK;
+}
+
+// One cached plan for the host compact entry point, reused while the geometry is unchanged.
+static std::mutex g_cache_mu;
+static img2d_plan *g_cached = nullptr;
+static std::vector<int> g_cached_key;
+
+}  // namespace img2d
+
+using namespace img2d;
+
+extern "C" {
+
+const char *img2d_last_error(void) { return g_err.c_str(); }
+
+int img2d_version(void) { return 10000; }
+
+int img2d_extrapolate_host_order(int ns, int nextrap, int nz, int nx, int nf, int nt, int M,
+                                 const img2d_c64 *op_forw, const img2d_c64 *op_back,
+                                 img2d_c64 *wave_fs, img2d_c64 *shot_fs, float *image)
+{
+    return run_dense(ns, nextrap, nz, nx, nf, nt, M, (const cpx *)op_forw, (const cpx *)op_back,
+                     (cpx *)wave_fs, (cpx *)shot_fs, image, 1);
+}
+
+int img2d_extrapolate_device_order(int ns, int nextrap, int nz, int nt, int nf, int nx, int M,
+                                   const img2d_c64 *op_forw, img2d_c64 *forw_pulse,
+                                   const img2d_c64 *op_back, img2d_c64 *back_pulse, float *image,
+                                   int write_back)
+{
+    return run_dense(ns, nextrap, nz, nx, nf, nt, M, (const cpx *)op_forw, (const cpx *)op_back,
+                     (cpx *)forw_pulse, (cpx *)back_pulse, image, write_back);
+}
+
+int img2d_plan_create(img2d_plan **plan, int ns, int nextrap, int nz, int nx, int nf, int nt, int M,
+                      int nk, const int *shot_x0, const int *shot_nx, int flags)
+{
+    if (!plan) return fail(IMG2D_EINVAL, "plan pointer is NULL");
+    *plan = nullptr;
+    int rc;
+    if ((rc = check_device())) return rc;
+    img2d_plan *p = new img2d_plan();
+    const int mode = (flags & IMG2D_FLAG_TWO_TABLES) ? OP_TWO : OP_CONJ;
+    if ((rc = build_plan(p, ns, nextrap, nz, nx, nf, nt, M, nk, shot_x0, shot_nx, flags, mode))) {
+        delete p;
+        return rc;
+    }
+    *plan = p;
+    return IMG2D_OK;
+}
+
+int img2d_plan_set_model(img2d_plan *p, const double *d_omega, const double *d_velocity, double dk,
+                         const img2d_c64 *d_tab_forw, const img2d_c64 *d_tab_back, void *stream)
+{
+    if (!p) return fail(IMG2D_EINVAL, "plan is NULL");
+    return set_model(p, d_omega, d_velocity, dk, (const cpx *)d_tab_forw, (const cpx *)d_tab_back,
+                     (cudaStream_t)stream);
+}
+
+int img2d_plan_execute(img2d_plan *p, img2d_c64 *d_wave, img2d_c64 *d_shot, float *d_image,
+                       float *d_image_shots, void *stream)
+{
+    if (!p) return fail(IMG2D_EINVAL, "plan is NULL");
+    if (!d_wave || !d_shot) return fail(IMG2D_EINVAL, "wavefield pointers are NULL");
+    MigrateArgs a = base_args(p, (cpx *)d_wave, (cpx *)d_shot);
+    return launch(p, a, d_image, d_image_shots, (long long)p->nz * p->nx, (cudaStream_t)stream);
+}
+
+long long img2d_plan_shot_offset(const img2d_plan *p, int s)
+{
+    if (!p || s < 0 || s >= p->ns) return -1;
+    return p->off[s];
+}
+
+long long img2d_plan_wavefield_elems(const img2d_plan *p) { return p ? p->wave_elems : -1; }
+
+size_t img2d_plan_workspace_bytes(const img2d_plan *p)
+{
+    if (!p) return 0;
+    return p->items.bytes + p->groups.bytes + p->group_shots.bytes + p->shot_win.bytes + p->shot_off.bytes +
+           p->idx.bytes + p->tabF.bytes + p->tabB.bytes + p->partial.bytes + p->comp.bytes + p->counter.bytes +
+           p->naive_buf.bytes;
+}
+
+int img2d_plan_describe(const img2d_plan *p, char *buf, int buflen)
+{
+    if (!p || !buf || buflen <= 0) return fail(IMG2D_EINVAL, "bad describe arguments");
+    snprintf(buf, buflen,
+             "{\"kernel\": \"%s\", \"G\": %d, \"X\": %d, \"L\": %d, \"grid\": %d, \"block\": 256, "
+             "\"smem\": %zu, \"items\": %d, \"max_union_width\": %d, \"mode\": %d}",
+             p->fixed ? "migrate_fixed" : "migrate_generic", p->G, p->fixed ? kX : 4, p->L, p->grid, p->smem,
+             p->n_items, p->max_w, p->mode);
+    return IMG2D_OK;
+}
+
+void img2d_plan_destroy(img2d_plan *p) { delete p; }
+
+int img2d_plan_kernel_ms(img2d_plan *p, float *ms)
+{
+    if (!p || !ms) return fail(IMG2D_EINVAL, "bad arguments");
+    if (!p->ev_recorded) return fail(IMG2D_EINVAL, "no kernel launched on this plan yet");
+    IMG2D_CUDA(cudaEventSynchronize(p->ev1));
+    IMG2D_CUDA(cudaEventElapsedTime(ms, p->ev0, p->ev1));
+    return IMG2D_OK;
+}
+
+int img2d_measure_fp32_peak(double *tflops)
+{
+    if (!tflops) return fail(IMG2D_EINVAL, "tflops is NULL");
+    int rc;
+    if ((rc = check_device())) return rc;
+    int dev = 0, nsm = 0;
+    IMG2D_CUDA(cudaGetDevice(&dev));
+    IMG2D_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    Scratch sc;
+    float *out;
+    const int blocks = nsm * 4, threads = 512, iters = 4096;
+    if ((rc = sc.alloc(&out, (size_t)blocks * threads * sizeof(float)))) return rc;
+    fma_probe_kernel<<<blocks, threads>>>(out, 64);
+    IMG2D_CUDA(cudaGetLastError());
+    cudaEvent_t e0, e1;
+    IMG2D_CUDA(cudaEventCreate(&e0));
+    IMG2D_CUDA(cudaEventCreate(&e1));
+    float best = 1e30f;
+    for (int r = 0; r < 3; ++r) {
+        cudaEventRecord(e0);
+        fma_probe_kernel<<<blocks, threads>>>(out, iters);
+        cudaEventRecord(e1);
+        cudaError_t e = cudaEventSynchronize(e1);
+        if (e != cudaSuccess) {
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+            return fail(IMG2D_ECUDA, std::string("fma probe: ") + cudaGetErrorString(e));
+        }
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        best = std::min(best, ms);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    // 16 chains x 8 FMAs per iteration per thread, 2 flops per FMA
+    *tflops = 2.0 * 128.0 * iters * (double)blocks * threads / (best * 1e-3) * 1e-12;
+    return IMG2D_OK;
+}
+
+int img2d_plan_execute_naive(img2d_plan *p, img2d_c64 *d_wave, img2d_c64 *d_shot, float *d_image,
+                             void *stream)
+{
+    if (!p) return fail(IMG2D_EINVAL, "plan is NULL");
+    if (p->mode != OP_CONJ) return fail(IMG2D_EINVAL, "naive form supports the single-table mode only");
+    if (!d_wave || !d_shot || !d_image) return fail(IMG2D_EINVAL, "null device pointer");
+    cudaStream_t st = (cudaStream_t)stream;
+    const int M = p->M;
+    const int maxw = *std::max_element(p->w.begin(), p->w.end());
+    int rc;
+    if ((rc = p->naive_buf.ensure(2 * (size_t)(maxw + 2 * M) * sizeof(float4)))) return rc;
+    float4 *b0 = p->naive_buf.as<float4>(), *b1 = b0 + (maxw + 2 * M);
+    IMG2D_CUDA(cudaMemsetAsync(d_image, 0, (size_t)p->nextrap * p->nx * sizeof(float), st));
+    for (int s = 0; s < p->ns; ++s) {
+        const int w = p->w[s], x0 = p->x0[s];
+        const int blocks = (w + 127) / 128;
+        for (int j = 0; j < p->nf; ++j) {
+            IMG2D_CUDA(cudaMemsetAsync(b0, 0, 2 * (size_t)(maxw + 2 * M) * sizeof(float4), st));
+            cpx *ws = (cpx *)d_wave + p->off[s] + (long long)j * w;
+            cpx *rs = (cpx *)d_shot + p->off[s] + (long long)j * w;
+            naive_pack_kernel<<<blocks, 128, 0, st>>>(ws, rs, w, M, b0, 1);
+            float4 *cur = b0, *nxt = b1;
+            for (int l = 0; l < p->nextrap; ++l) {
+                const uint16_t *idx_row = p->idx.as<uint16_t>() + ((long long)j * p->nextrap + l) * p->idx_lstride;
+                naive_step_kernel<<<blocks, 128, 0, st>>>(cur, nxt, w, M, p->tabF.as<cpx>(), p->tab_stride, idx_row,
+                                                          x0, d_image + (long long)l * p->nx);
+                std::swap(cur, nxt);
+            }
+            naive_unpack_kernel<<<blocks, 128, 0, st>>>(cur, w, M, ws, rs);
+        }
+    }
+    IMG2D_CUDA(cudaGetLastError());
+    return IMG2D_OK;
+}
+
+int img2d_migrate_compact(int ns, int nextrap, int nz, int nx, int nf, int nt, int M, int nk, double dk,
+                          const double *omega, const double *velocity, const img2d_c64 *tab_forw,
+                          const img2d_c64 *tab_back, const int *shot_x0, const int *shot_nx,
+                          img2d_c64 *wave_fs, img2d_c64 *shot_fs, float *image, float *image_shots, int flags)
+{
+    int rc;
+    if ((rc = check_device())) return rc;
+    if (!omega || !velocity || !tab_forw || !wave_fs || !shot_fs)
+        return fail(IMG2D_EINVAL, "null pointer argument");
+    if ((flags & IMG2D_FLAG_TWO_TABLES) && !tab_back) return fail(IMG2D_EINVAL, "two-table mode needs tab_back");
+    std::lock_guard<std::mutex> lock(g_cache_mu);
+    std::vector<int> key = {ns, nextrap, nz, nx, nf, nt, M, nk, flags};
+    for (int s = 0; s < ns; ++s) {
+        key.push_back(shot_x0 ? shot_x0[s] : 0);
+        key.push_back(shot_nx ? shot_nx[s] : nx);
+    }
+    if (!g_cached || key != g_cached_key) {
+        delete g_cached;
+        g_cached = nullptr;
+        g_cached_key.clear();
+        img2d_plan *p = nullptr;
+        if ((rc = img2d_plan_create(&p, ns, nextrap, nz, nx, nf, nt, M, nk, shot_x0, shot_nx, flags))) return rc;
+        g_cached = p;
+        g_cached_key = key;
+    }
+    img2d_plan *p = g_cached;
+    Scratch sc;
+    const size_t L = 2 * (size_t)M + 1;
+    const size_t plane = (size_t)nz * nx;
+    double *dO, *dV;
+    cpx *dTF, *dTB = nullptr, *dW, *dS;
+    float *dI = nullptr, *dIS = nullptr;
+    if ((rc = sc.alloc(&dO, nf * sizeof(double)))) return rc;
+    if ((rc = sc.alloc(&dV, (size_t)nextrap * nx * sizeof(double)))) return rc;
+    if ((rc = sc.alloc(&dTF, nk * L * sizeof(cpx)))) return rc;
+    if ((flags & IMG2D_FLAG_TWO_TABLES) && (rc = sc.alloc(&dTB, nk * L * sizeof(cpx)))) return rc;
+    if ((rc = sc.alloc(&dW, p->wave_elems * sizeof(cpx)))) return rc;
+    if ((rc = sc.alloc(&dS, p->wave_elems * sizeof(cpx)))) return rc;
+    if (image && (rc = sc.alloc(&dI, (size_t)nextrap * nx * sizeof(float)))) return rc;
+    if (image_shots && (rc = sc.alloc(&dIS, (size_t)ns * plane * sizeof(float)))) return rc;
+    IMG2D_CUDA(cudaMemcpy(dO, omega, nf * sizeof(double), cudaMemcpyHostToDevice));
+    IMG2D_CUDA(cudaMemcpy(dV, velocity, (size_t)nextrap * nx * sizeof(double), cudaMemcpyHostToDevice));
+    IMG2D_CUDA(cudaMemcpy(dTF, tab_forw, nk * L * sizeof(cpx), cudaMemcpyHostToDevice));
+    if (dTB) IMG2D_CUDA(cudaMemcpy(dTB, tab_back, nk * L * sizeof(cpx), cudaMemcpyHostToDevice));
+    IMG2D_CUDA(cudaMemcpy(dW, wave_fs, p->wave_elems * sizeof(cpx), cudaMemcpyHostToDevice));
+    IMG2D_CUDA(cudaMemcpy(dS, shot_fs, p->wave_elems * sizeof(cpx), cudaMemcpyHostToDevice));
+    if ((rc = set_model(p, dO, dV, dk, dTF, dTB, 0))) return rc;
+    MigrateArgs a = base_args(p, dW, dS);
+    if ((rc = launch(p, a, dI, dIS, (long long)plane, 0))) return rc;
+    IMG2D_CUDA(cudaDeviceSynchronize());
+    if (image) IMG2D_CUDA(cudaMemcpy(image, dI, (size_t)nextrap * nx * sizeof(float), cudaMemcpyDeviceToHost));
+    if (image_shots)
+        IMG2D_CUDA(cudaMemcpy2D(image_shots, plane * sizeof(float), dIS, plane * sizeof(float),
+                                (size_t)nextrap * nx * sizeof(float), ns, cudaMemcpyDeviceToHost));
+    IMG2D_CUDA(cudaMemcpy(wave_fs, dW, p->wave_elems * sizeof(cpx), cudaMemcpyDeviceToHost));
+    IMG2D_CUDA(cudaMemcpy(shot_fs, dS, p->wave_elems * sizeof(cpx), cudaMemcpyDeviceToHost));
+    return IMG2D_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,130 @@
+/*
+ * imaging2d_wlsq_b200.h -- C ABI of the B200 extrapolation + imaging library.
+ *
+ * Library: imaging2d_wlsq_b200/libimaging2d_wlsq_b200.so (CUDA, sm_100a).
+ * Drop-in shims with the reference's library names and its void `extrapolate` symbols are
+ * built into imaging2d_wlsq_b200/dropin/ (see INTEGRATION.md).
+ *
+ * Data conventions shared by every entry point:
+ *   img2d_c64   interleaved (re, im) float32 pair, the layout of numpy.complex64 and of the
+ *               reference's `fcomp` = thrust::complex<float> (cpp_src/types.h:9).
+ *   All arrays are C-contiguous.  Host-pointer entry points copy to and from the current CUDA
+ *   device inside the call and return when the results are back in host memory.
+ *   Every int-returning function returns IMG2D_OK (0) or an IMG2D_E* code; the text of the last
+ *   failure on the calling thread is available from img2d_last_error().
+ */
+#ifndef IMAGING2D_WLSQ_B200_H
+#define IMAGING2D_WLSQ_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct {
+    float re, im;
+} img2d_c64;
+
+#define IMG2D_OK 0
+#define IMG2D_EINVAL 1   /* invalid dimensions or pointers */
+#define IMG2D_ENOMEM 2   /* device allocation failed */
+#define IMG2D_ECUDA 3    /* a CUDA runtime call or kernel launch failed */
+#define IMG2D_ENODEV 4   /* no CUDA device visible */
+
+/* flags for the compact-table entry points */
+#define IMG2D_FLAG_TWO_TABLES 1   /* use tab_back for the receiver instead of conj(tab_forw) */
+#define IMG2D_FLAG_GENERIC 2      /* force the runtime-length kernel (testing) */
+
+const char *img2d_last_error(void);
+int img2d_version(void);
+
+/* ------------------------------------------------------------------------------------------
+ * Drop-in entry points: the reference's dense-table ABI.
+ * opF/opB are dense operator tables (nextrap, nf, nx, 2M+1); wavefields are (ns, nt, nx) with the
+ * first nf rows used; image is (ns, nz, nx) float32 and rows [0, nextrap) of every shot are
+ * overwritten with Re(sum_w S conj R).
+ * ---------------------------------------------------------------------------------------- */
+
+/* Replaces `extrapolate` and `extrapolate_v0` of cpp_src/extrapolation_cpu.cpp:11-14 and :115-118
+ * (bound in cpp_src/interface.py:50-70).  Host argument order.  wave_fs and shot_fs are
+ * overwritten with the final-depth wavefields (extrapolation_cpu.cpp:91-99). */
+int img2d_extrapolate_host_order(int ns, int nextrap, int nz, int nx, int nf, int nt, int M,
+                                 const img2d_c64 *op_forw, const img2d_c64 *op_back,
+                                 img2d_c64 *wave_fs, img2d_c64 *shot_fs, float *image);
+
+/* Replaces `extrapolate` of cpp_src/extrapolation_gpu.cu:74-76 (write_back = 0, that library does
+ * not write the wavefields back), cpp_src/extrapolation_revOp_gpu.cu:78-80 and
+ * cpp_src/extrapolation_sh_revOp_gpu.cu:87-89 (write_back = 1), bound in
+ * cpp_src/interface_cuda.py:17-52.  Device argument order.  With write_back the final-depth
+ * wavefields go to forw_pulse/back_pulse with shot stride nt*nx. */
+int img2d_extrapolate_device_order(int ns, int nextrap, int nz, int nt, int nf, int nx, int M,
+                                   const img2d_c64 *op_forw, img2d_c64 *forw_pulse,
+                                   const img2d_c64 *op_back, img2d_c64 *back_pulse, float *image,
+                                   int write_back);
+
+/* ------------------------------------------------------------------------------------------
+ * Compact-table entry point (replaces the dense-table gather of
+ * py_src/operatorsPreparation/preparation.py:101-115 followed by the call of main.py:153-160).
+ *   omega[nf]            angular frequencies w[j] (float64)
+ *   velocity[nz*nx]      velocity model (float64), rows [0, nextrap) used
+ *   tab_forw[nk*(2M+1)]  row i = forward WLSQ operator for kappa[i] = i*dk
+ *   tab_back             row i = receiver operator, read only with IMG2D_FLAG_TWO_TABLES
+ *   shot_x0, shot_nx     per-shot aperture [x0, x0+nx_s) inside [0, nx); NULL = full aperture
+ *   wave_fs, shot_fs     packed per-shot blocks of nt rows x nx_s samples (first nf rows used),
+ *                        blocks in shot order; overwritten with the final-depth wavefields
+ *   image[nz*nx]         stacked image (sum over shots), rows [0, nextrap) overwritten; may be NULL
+ *   image_shots          per-shot images (ns, nz, nx), rows [0, nextrap) overwritten; may be NULL
+ * The operator for (depth l, frequency j, position x) is row find_nearest(kappa, w[j]/v[l,x])
+ * (py_src/operatorsPreparation/util.py:5-8), evaluated in float64 on the device.
+ * ---------------------------------------------------------------------------------------- */
+int img2d_migrate_compact(int ns, int nextrap, int nz, int nx, int nf, int nt, int M, int nk,
+                          double dk, const double *omega, const double *velocity,
+                          const img2d_c64 *tab_forw, const img2d_c64 *tab_back,
+                          const int *shot_x0, const int *shot_nx, img2d_c64 *wave_fs,
+                          img2d_c64 *shot_fs, float *image, float *image_shots, int flags);
+
+/* ------------------------------------------------------------------------------------------
+ * Plan interface for device-resident data (the building block under the host entry points).
+ * A plan fixes the geometry (dimensions, apertures) and owns its device workspace.
+ * ---------------------------------------------------------------------------------------- */
+typedef struct img2d_plan img2d_plan;
+
+int img2d_plan_create(img2d_plan **plan, int ns, int nextrap, int nz, int nx, int nf, int nt,
+                      int M, int nk, const int *shot_x0, const int *shot_nx, int flags);
+/* Device pointers.  Copies the tables into the plan (rows padded for 16-byte loads) and builds
+ * the operator index table for (omega, velocity, dk).  stream: cudaStream_t or NULL. */
+int img2d_plan_set_model(img2d_plan *plan, const double *d_omega, const double *d_velocity,
+                         double dk, const img2d_c64 *d_tab_forw, const img2d_c64 *d_tab_back,
+                         void *stream);
+/* Device pointers, packed layout of img2d_migrate_compact.  Asynchronous on `stream`. */
+int img2d_plan_execute(img2d_plan *plan, img2d_c64 *d_wave, img2d_c64 *d_shot, float *d_image,
+                       float *d_image_shots, void *stream);
+/* Element offset of shot s's block inside the packed wavefield arrays, and their total size. */
+long long img2d_plan_shot_offset(const img2d_plan *plan, int s);
+long long img2d_plan_wavefield_elems(const img2d_plan *plan);
+/* Device bytes held by the plan, and the kernel configuration it chose. */
+size_t img2d_plan_workspace_bytes(const img2d_plan *plan);
+int img2d_plan_describe(const img2d_plan *plan, char *buf, int buflen);
+void img2d_plan_destroy(img2d_plan *plan);
+
+/* Device time (ms) of the persistent migration kernel alone in the last img2d_plan_execute on this
+ * plan, from CUDA events recorded around that launch on its stream (waits for it to finish). */
+int img2d_plan_kernel_ms(img2d_plan *plan, float *ms);
+
+/* FP32 FMA throughput of the current device in TFLOP/s, measured by a short kernel of independent
+ * FMA chains (the denominator of the FP32 roofline; not part of the migration path). */
+int img2d_measure_fp32_peak(double *tflops);
+
+/* Naive comparison form: one kernel launch per (shot, frequency, depth), operators from the
+ * compact table, wavefields in global memory.  Same arguments and results as
+ * img2d_plan_execute (device pointers).  Used only to measure the batched kernel against. */
+int img2d_plan_execute_naive(img2d_plan *plan, img2d_c64 *d_wave, img2d_c64 *d_shot,
+                             float *d_image, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* IMAGING2D_WLSQ_B200_H */

@@ -1,0 +1,211 @@
+"""GPU parity: the CUDA library through its C ABI against the reference's known answers, the CPU
+oracle (FP32 reference-order and FP64) and the reference demo.  Tolerances:
+  known answers            1e-5 absolute, as the reference's own tests (test_cpp_src.py:13)
+  dense ABI vs FP32 oracle  max |diff| <= 1e-5 * max|image| and wavefields likewise
+  compact vs FP64 oracle    relative L2 of the image <= 1e-5 (single-table mode adds the
+                            conj(T_forw) vs T_back rounding, still inside 1e-5)
+"""
+import ctypes
+import os
+
+import numpy as np
+import pytest
+from numpy.ctypeslib import ndpointer
+
+from imaging2d_wlsq_b200 import DROPIN_DIR, interface, interface_cuda, migration, synthetic
+from oracle import oracle
+from tests import kat_cases as K
+from tests.conftest import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+HOST_CASES = K.cpu_cases() + [c[:7] for c in K.gpu_cases()] + K.py_float_cases()
+
+
+def _host_call(fn, d, f, b, pf, pb):
+    img = np.zeros((d["ns"], d["nz"], d["nx"]), dtype=np.float32)
+    w, s = pf.copy(), pb.copy()
+    fn(d["ns"], d["nextrap"], d["nz"], d["nx"], d["nf"], d["nt"], d["M"], f, b, w, s, img)
+    return img, w, s
+
+
+def _dev_call(fn, d, f, b, pf, pb):
+    img = np.zeros((d["ns"], d["nz"], d["nx"]), dtype=np.float32)
+    w, s = pf.copy(), pb.copy()
+    fn(d["ns"], d["nextrap"], d["nz"], d["nt"], d["nf"], d["nx"], d["M"], f, w, b, s, img)
+    return img, w, s
+
+
+def _dropin(name, symbol="extrapolate"):
+    # bound exactly as the reference's cpp_src/interface.py / interface_cuda.py bind it
+    lib = ctypes.CDLL(os.path.join(DROPIN_DIR, name))
+    f = getattr(lib, symbol)
+    f.restype = ctypes.c_void_p
+    f.argtypes = [ctypes.c_int] * 7 + [ndpointer(dtype=np.complex64, flags=("C", "A"))] * 4 + \
+        [ndpointer(dtype=np.float32, flags=("C", "A"))]
+    return f
+
+
+@pytest.mark.parametrize("case", HOST_CASES, ids=[c[0] for c in HOST_CASES])
+def test_known_answers_host_order(case):
+    name, d, f, b, pf, pb, exp = case
+    for fn in (interface.extrapolate, interface.extrapolate_v0, _dropin("extrapolation_cpu.so"),
+               _dropin("extrapolation_cpu.so", "extrapolate_v0")):
+        img, _, _ = _host_call(fn, d, f, b, pf, pb)
+        ok, msg = K.check_image(img[0], exp, d["nz"], d["nx"])
+        assert ok, f"{name}: {msg}"
+
+
+@pytest.mark.parametrize("case", K.gpu_cases(), ids=[c[0] for c in K.gpu_cases()])
+def test_known_answers_device_order(case):
+    name, d, f, b, pf, pb, exp, waves = case
+    (pi, pv), (ri, rv) = waves["pulse"], waves["pulse2"]
+    for fn, wb in ((interface_cuda.extrapolate, False), (interface_cuda.extrapolate_revOp, True),
+                   (interface_cuda.extrapolate_sh_revOp, True), (_dropin("extrapolation_gpu.so"), False),
+                   (_dropin("extrapolation_revOp_gpu.so"), True), (_dropin("extrapolation_sh_revOp_gpu.so"), True)):
+        img, w, s = _dev_call(fn, d, f, b, pf, pb)
+        ok, msg = K.check_image(img[0], exp, d["nz"], d["nx"])
+        assert ok, f"{name}: {msg}"
+        if wb:
+            assert abs(w[pi] - pv) <= K.SDELTA and abs(s[ri] - rv) <= K.SDELTA, name
+        else:
+            np.testing.assert_array_equal(w, pf)  # extrapolation_gpu.cu never writes wavefields back
+            np.testing.assert_array_equal(s, pb)
+
+
+def _rand_dense(ns, nextrap, nz, nx, nf, nt, M, seed):
+    rng = np.random.default_rng(seed)
+    L = 2 * M + 1
+
+    def c(*shape):
+        return (rng.standard_normal(shape) + 1j * rng.standard_normal(shape)).astype(np.complex64)
+
+    return c(nextrap, nf, nx, L) * (0.6 / np.sqrt(L)), c(nextrap, nf, nx, L) * (0.6 / np.sqrt(L)), c(ns, nt, nx), c(ns, nt, nx)
+
+
+@pytest.mark.parametrize("ns,nextrap,nz,nx,nf,nt,M", [
+    (1, 3, 5, 17, 5, 7, 2), (3, 6, 8, 40, 6, 6, 5), (5, 4, 4, 33, 9, 12, 12), (9, 7, 9, 150, 11, 11, 21),
+    (2, 2, 3, 1, 2, 2, 1), (4, 5, 6, 64, 3, 3, 0), (16, 3, 3, 96, 4, 4, 7)])
+def test_dense_abi_matches_oracle(ns, nextrap, nz, nx, nf, nt, M):
+    f, b, pf, pb = _rand_dense(ns, nextrap, nz, nx, nf, nt, M, ns * 1000 + nx)
+    d = dict(ns=ns, nextrap=nextrap, nz=nz, nx=nx, nf=nf, nt=nt, M=M)
+    img_o = np.full((ns, nz, nx), 7.0, dtype=np.float32)
+    wo, so = pf.copy(), pb.copy()
+    oracle.extrapolate_f32(ns, nextrap, nz, nx, nf, nt, M, f, b, wo, so, img_o)
+    img_g = np.full((ns, nz, nx), 7.0, dtype=np.float32)
+    wg, sg = pf.copy(), pb.copy()
+    interface.extrapolate(ns, nextrap, nz, nx, nf, nt, M, f, b, wg, sg, img_g)
+    scale = np.abs(img_o[:, :nextrap]).max()
+    assert np.abs(img_g - img_o).max() <= 1e-5 * scale + 1e-6
+    assert np.all(img_g[:, nextrap:] == 7.0)  # rows >= nextrap untouched
+    for g, o in ((wg, wo), (sg, so)):
+        assert np.abs(g - o).max() <= 1e-5 * np.abs(o).max() + 1e-6
+        np.testing.assert_array_equal(g[:, nf:], pf[:, nf:] if g is wg else pb[:, nf:])  # rows >= nf untouched
+
+
+def _compact_check(w, img, wave, shot, two_tables=False, tol=1e-5):
+    tab_b = None
+    if two_tables:
+        tab_b = w.table_back
+    stack, _, wo, so = oracle.migrate_workload_f64(w, tab_back=tab_b)
+    e_img = rel_l2(img, stack)
+    e_w = rel_l2(wave, wo)
+    e_s = rel_l2(shot, so)
+    assert e_img <= tol, f"image rel-L2 {e_img:.2e}"
+    assert e_w <= tol and e_s <= tol, f"wavefield rel-L2 {e_w:.2e} {e_s:.2e}"
+    return e_img
+
+
+@pytest.mark.parametrize("maker,scale", [(synthetic.plain_small, 0.5), (synthetic.plain_medium, 0.125),
+                                         (synthetic.batched_uneven, 0.1), (synthetic.precision, 0.05)])
+def test_compact_matches_fp64_oracle(maker, scale):
+    w = maker(scale=scale)
+    img, _, wave, shot = migration.migrate_workload(w)
+    _compact_check(w, img, wave, shot)
+
+
+def test_compact_generic_kernel_and_per_shot_images():
+    w = synthetic.batched_uneven(scale=0.08)
+    img, imgs, wave, shot = migration.migrate_workload(w, image_shots=True, generic=True)
+    _compact_check(w, img, wave, shot)
+    _, shots_o, _, _ = oracle.migrate_workload_f64(w)
+    assert rel_l2(imgs, shots_o) <= 1e-5
+    # per-shot images are zero outside each shot's aperture
+    for s in range(w.ns):
+        x0, n = int(w.shot_x0[s]), int(w.shot_nx[s])
+        assert np.all(imgs[s, :, :x0] == 0) and np.all(imgs[s, :, x0 + n:] == 0)
+    # stack == sum of per-shot images
+    assert rel_l2(imgs.sum(axis=0), img) <= 1e-6
+
+
+def test_compact_two_tables():
+    from imaging2d_wlsq_b200 import operators as ops
+    w = synthetic.plain_small(scale=0.4)
+    w.table_back = ops.design_compact_table(w.nx, w.dx, w.dz, w.M, w.nk, w.dk, back=True)
+    img, _, wave, shot = migration.migrate_workload(w, two_tables=True, table_back=w.table_back)
+    _compact_check(w, img, wave, shot, two_tables=True)
+
+
+def test_demo_matches_reference(golden_demo):
+    g = golden_demo
+    ns = g["src"].shape[0]
+    nz, nx, nw, M, nk = (int(g[k]) for k in ("nz", "nx", "nw", "M", "nk"))
+    for two in (True, False):
+        wave, shot = g["src"].reshape(-1).copy(), g["rec"].reshape(-1).copy()
+        img, _ = migration.migrate(ns, int(g["nextrap"]), nz, nx, nw, nw, M, nk, float(g["dk"]), g["omega"],
+                                   g["velocity"], g["tab_f"], wave, shot, tab_back=g["tab_b"], two_tables=two)
+        assert rel_l2(img, g["image_ref_cpu"]) <= 1e-5, two
+        assert rel_l2(img, g["image_shipped"]) <= 3e-5, two
+        assert np.all(img[int(g["nextrap"]):] == 0)
+
+
+def test_plan_device_resident_matches_host_entry():
+    import torch
+    w = synthetic.batched_uneven(scale=0.08)
+    img_h, _, wave_h, shot_h = migration.migrate_workload(w)
+    plan = migration.Plan.for_workload(w)
+    dev = torch.device("cuda")
+    om = torch.from_numpy(w.omega).to(dev)
+    vel = torch.from_numpy(np.ascontiguousarray(w.velocity)).to(dev)
+    tab = torch.from_numpy(w.table).to(dev)
+    wave = torch.from_numpy(w.wave.copy()).to(dev)
+    shot = torch.from_numpy(w.shot.copy()).to(dev)
+    img = torch.zeros((w.nz, w.nx), dtype=torch.float32, device=dev)
+    plan.set_model(om, vel, w.dk, tab)
+    plan.execute(wave, shot, img)
+    torch.cuda.synchronize()
+    assert rel_l2(img.cpu().numpy(), img_h) <= 1e-6
+    assert rel_l2(wave.cpu().numpy(), wave_h) <= 1e-6
+    d = plan.describe()
+    assert d["G"] >= 1 and d["grid"] >= 1
+    plan.close()
+
+
+def test_naive_form_matches_batched():
+    import torch
+    w = synthetic.plain_medium(scale=0.06)
+    dev = torch.device("cuda")
+    plan = migration.Plan.for_workload(w)
+    plan.set_model(torch.from_numpy(w.omega).to(dev), torch.from_numpy(np.ascontiguousarray(w.velocity)).to(dev),
+                   w.dk, torch.from_numpy(w.table).to(dev))
+    out = []
+    for naive in (False, True):
+        wave = torch.from_numpy(w.wave.copy()).to(dev)
+        shot = torch.from_numpy(w.shot.copy()).to(dev)
+        img = torch.zeros((w.nz, w.nx), dtype=torch.float32, device=dev)
+        (plan.execute_naive if naive else plan.execute)(wave, shot, img)
+        torch.cuda.synchronize()
+        out.append((img.cpu().numpy(), wave.cpu().numpy()))
+    assert rel_l2(out[1][0], out[0][0]) <= 1e-5
+    assert rel_l2(out[1][1], out[0][1]) <= 1e-5
+    plan.close()
+
+
+def test_invalid_arguments_raise():
+    from imaging2d_wlsq_b200 import LibraryError
+    w = synthetic.plain_small(scale=0.2)
+    with pytest.raises(LibraryError):
+        migration.Plan(w.ns, w.nextrap, w.nz, w.nx, w.nf, w.nt, w.M, w.nk, shot_x0=[0, 0, 0, w.nx - 1],
+                       shot_nx=[w.nx] * 4)
+    with pytest.raises(LibraryError):
+        migration.Plan(w.ns, w.nz + 1, w.nz, w.nx, w.nf, w.nt, w.M, w.nk)
