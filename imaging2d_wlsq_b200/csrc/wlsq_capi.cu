@@ -192,8 +192,8 @@ struct img2d_plan {
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
     }
-    img2d::DevBuf items, groups, group_shots, shot_win, shot_off, idx, tabF, tabB, partial, comp,
-        counter, naive_buf;
+    int n_slots = 0;
+    img2d::DevBuf items, groups, segs, owner, shot_off, idx, tabF, tabB, partial, comp, counter, naive_buf;
     // dense tables (drop-in ABI) are owned by the caller of run_dense
 };
 
@@ -228,6 +228,7 @@ static int build_plan(img2d_plan *p, int ns, int nextrap, int nz, int nx, int nf
     if (mode != OP_DENSE && (nk <= 0 || nk > 65535))
         return fail(IMG2D_EINVAL, "nk must be in [1, 65535]");
     if ((long long)nf * nextrap * nx > (1ll << 40)) return fail(IMG2D_EINVAL, "problem too large");
+    if (ns > 32767) return fail(IMG2D_EINVAL, "at most 32767 shots per plan");
     p->ns = ns; p->nextrap = nextrap; p->nz = nz; p->nx = nx; p->nf = nf; p->nt = nt; p->M = M;
     p->L = 2 * M + 1; p->nk = nk; p->flags = flags; p->mode = mode;
     p->x0.assign(ns, 0);
@@ -267,27 +268,69 @@ static int build_plan(img2d_plan *p, int ns, int nextrap, int nz, int nx, int nf
     p->fixed = use_fixed;
     p->fn = use_fixed ? find_fixed(G, p->L) : find_generic(G, mode);
 
-    // Group shots of similar aperture: sort by (x0, x1) and take consecutive runs of G.
+    // Pack shots into lane slots: shots sorted by aperture start go to the slot whose last shot
+    // ends furthest to the left while still leaving >= M zero samples before this one (interval
+    // colouring, best fit); full-aperture shots get a slot each.  Then slots of similar extent
+    // form groups of G that share a work item.
     std::vector<int> order(ns);
     std::iota(order.begin(), order.end(), 0);
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
         if (p->x0[a] != p->x0[b]) return p->x0[a] < p->x0[b];
-        return p->x0[a] + p->w[a] < p->x0[b] + p->w[b];
+        return p->w[a] < p->w[b];
     });
-    std::vector<int4> groups;
-    std::vector<int> gshots;
-    int widest = 0;
-    for (int g0 = 0; g0 < ns; g0 += G) {
-        int n = std::min(G, ns - g0), u0 = nx, u1 = 0;
-        for (int k = 0; k < n; ++k) {
-            int s = order[g0 + k];
-            u0 = std::min(u0, p->x0[s]);
-            u1 = std::max(u1, p->x0[s] + p->w[s]);
-            gshots.push_back(s);
+    std::vector<std::vector<int>> slots;
+    std::vector<int> slot_end;
+    for (int s : order) {
+        int best = -1;
+        for (size_t i = 0; i < slots.size(); ++i)
+            if (slot_end[i] + M <= p->x0[s] && (best < 0 || slot_end[i] > slot_end[best])) best = (int)i;
+        if (best < 0) {
+            slots.push_back({s});
+            slot_end.push_back(p->x0[s] + p->w[s]);
+        } else {
+            slots[best].push_back(s);
+            slot_end[best] = p->x0[s] + p->w[s];
         }
-        groups.push_back(make_int4(g0, n, u0, u1 - u0));
-        widest = std::max(widest, u1 - u0);
     }
+    std::vector<int> sorder(slots.size());
+    std::iota(sorder.begin(), sorder.end(), 0);
+    auto ext0 = [&](int i) { return p->x0[slots[i].front()]; };
+    std::stable_sort(sorder.begin(), sorder.end(), [&](int a, int b) {
+        if (ext0(a) != ext0(b)) return ext0(a) < ext0(b);
+        return slot_end[a] < slot_end[b];
+    });
+    std::vector<GroupDesc> groups;
+    std::vector<int4> segs;
+    std::vector<int16_t> owner;
+    int widest = 0;
+    for (size_t g0 = 0; g0 < sorder.size(); g0 += G) {
+        const int n = (int)std::min<size_t>(G, sorder.size() - g0);
+        int u0 = nx, u1 = 0;
+        for (int k = 0; k < n; ++k) {
+            const int i = sorder[g0 + k];
+            u0 = std::min(u0, ext0(i));
+            u1 = std::max(u1, slot_end[i]);
+        }
+        GroupDesc gd{};
+        gd.seg_begin = (int)segs.size();
+        gd.u0 = u0;
+        gd.W = u1 - u0;
+        gd.nslots = n;
+        gd.owner_stride = (gd.W + 7) / 8 * 8;
+        gd.owner_off = (long long)owner.size();
+        owner.resize(owner.size() + (size_t)n * gd.owner_stride, (int16_t)-1);
+        for (int k = 0; k < n; ++k) {
+            for (int s : slots[sorder[g0 + k]]) {
+                segs.push_back(make_int4(s, k, p->x0[s], p->w[s]));
+                int16_t *row = owner.data() + gd.owner_off + (size_t)k * gd.owner_stride;
+                for (int x = p->x0[s]; x < p->x0[s] + p->w[s]; ++x) row[x - u0] = (int16_t)s;
+            }
+        }
+        gd.nseg = (int)segs.size() - gd.seg_begin;
+        groups.push_back(gd);
+        widest = std::max(widest, gd.W);
+    }
+    p->n_slots = (int)slots.size();
     p->max_w = widest;
     p->smem = smem_bytes(G, widest, M, X);
     // Items (group, frequency), widest groups first so the tail of the queue is short work.
@@ -295,25 +338,23 @@ static int build_plan(img2d_plan *p, int ns, int nextrap, int nz, int nx, int nf
     items.reserve(groups.size() * (size_t)nf);
     std::vector<int> gorder(groups.size());
     std::iota(gorder.begin(), gorder.end(), 0);
-    std::stable_sort(gorder.begin(), gorder.end(), [&](int a, int b) { return groups[a].w > groups[b].w; });
+    std::stable_sort(gorder.begin(), gorder.end(), [&](int a, int b) { return groups[a].W > groups[b].W; });
     for (int g : gorder)
         for (int j = 0; j < nf; ++j) items.push_back(make_int2(g, j));
     p->n_items = (int)items.size();
     p->grid = std::min(p->n_items, nsm);
 
-    std::vector<int2> win(ns);
-    for (int s = 0; s < ns; ++s) win[s] = make_int2(p->x0[s], p->w[s]);
     int rc;
     if ((rc = p->items.ensure(items.size() * sizeof(int2)))) return rc;
-    if ((rc = p->groups.ensure(groups.size() * sizeof(int4)))) return rc;
-    if ((rc = p->group_shots.ensure(gshots.size() * sizeof(int)))) return rc;
-    if ((rc = p->shot_win.ensure(win.size() * sizeof(int2)))) return rc;
+    if ((rc = p->groups.ensure(groups.size() * sizeof(GroupDesc)))) return rc;
+    if ((rc = p->segs.ensure(segs.size() * sizeof(int4)))) return rc;
+    if ((rc = p->owner.ensure(owner.size() * sizeof(int16_t)))) return rc;
     if ((rc = p->shot_off.ensure(p->off.size() * sizeof(long long)))) return rc;
     if ((rc = p->counter.ensure(sizeof(int)))) return rc;
     IMG2D_CUDA(cudaMemcpy(p->items.p, items.data(), items.size() * sizeof(int2), cudaMemcpyHostToDevice));
-    IMG2D_CUDA(cudaMemcpy(p->groups.p, groups.data(), groups.size() * sizeof(int4), cudaMemcpyHostToDevice));
-    IMG2D_CUDA(cudaMemcpy(p->group_shots.p, gshots.data(), gshots.size() * sizeof(int), cudaMemcpyHostToDevice));
-    IMG2D_CUDA(cudaMemcpy(p->shot_win.p, win.data(), win.size() * sizeof(int2), cudaMemcpyHostToDevice));
+    IMG2D_CUDA(cudaMemcpy(p->groups.p, groups.data(), groups.size() * sizeof(GroupDesc), cudaMemcpyHostToDevice));
+    IMG2D_CUDA(cudaMemcpy(p->segs.p, segs.data(), segs.size() * sizeof(int4), cudaMemcpyHostToDevice));
+    IMG2D_CUDA(cudaMemcpy(p->owner.p, owner.data(), owner.size() * sizeof(int16_t), cudaMemcpyHostToDevice));
     IMG2D_CUDA(cudaMemcpy(p->shot_off.p, p->off.data(), p->off.size() * sizeof(long long), cudaMemcpyHostToDevice));
     IMG2D_CUDA(cudaFuncSetAttribute(p->fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->smem));
     const size_t plane = (size_t)nextrap * nx;
@@ -339,9 +380,9 @@ static MigrateArgs base_args(img2d_plan *p, cpx *wave, cpx *shot)
     a.tab_stride = p->tab_stride;
     a.n_items = p->n_items;
     a.items = p->items.as<int2>();
-    a.groups = p->groups.as<int4>();
-    a.group_shots = p->group_shots.as<int>();
-    a.shot_win = p->shot_win.as<int2>();
+    a.groups = p->groups.as<GroupDesc>();
+    a.segs = p->segs.as<int4>();
+    a.owner = p->owner.as<int16_t>();
     a.shot_off = p->shot_off.as<long long>();
     a.tabF = p->tabF.as<cpx>();
     a.tabB = p->mode == OP_TWO ? p->tabB.as<cpx>() : p->tabF.as<cpx>();
@@ -553,7 +594,7 @@ long long img2d_plan_wavefield_elems(const img2d_plan *p) { return p ? p->wave_e
 size_t img2d_plan_workspace_bytes(const img2d_plan *p)
 {
     if (!p) return 0;
-    return p->items.bytes + p->groups.bytes + p->group_shots.bytes + p->shot_win.bytes + p->shot_off.bytes +
+    return p->items.bytes + p->groups.bytes + p->segs.bytes + p->owner.bytes + p->shot_off.bytes +
            p->idx.bytes + p->tabF.bytes + p->tabB.bytes + p->partial.bytes + p->comp.bytes + p->counter.bytes +
            p->naive_buf.bytes;
 }
@@ -563,9 +604,9 @@ int img2d_plan_describe(const img2d_plan *p, char *buf, int buflen)
     if (!p || !buf || buflen <= 0) return fail(IMG2D_EINVAL, "bad describe arguments");
     snprintf(buf, buflen,
              "{\"kernel\": \"%s\", \"G\": %d, \"X\": %d, \"L\": %d, \"grid\": %d, \"block\": 256, "
-             "\"smem\": %zu, \"items\": %d, \"max_union_width\": %d, \"mode\": %d}",
+             "\"smem\": %zu, \"items\": %d, \"slots\": %d, \"max_union_width\": %d, \"mode\": %d}",
              p->fixed ? "migrate_fixed" : "migrate_generic", p->G, p->fixed ? kX : 4, p->L, p->grid, p->smem,
-             p->n_items, p->max_w, p->mode);
+             p->n_items, p->n_slots, p->max_w, p->mode);
     return IMG2D_OK;
 }
 

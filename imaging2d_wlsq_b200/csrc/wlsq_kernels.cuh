@@ -9,11 +9,12 @@
 //   py_src/operatorsPreparation/preparation.py:101-115 the dense table is a gather of a compact
 //                                        (nk, 2M+1) table by idx = find_nearest(kappa, w/v(z,x)).
 //
-// Work decomposition (B200): one CTA owns one work item = (group of G shots, one frequency)
+// Work decomposition (B200): one CTA owns one work item = (group of G lane slots, one frequency)
 // for the whole depth loop; both wavefields of every shot of the group stay resident in shared
-// memory (ping-pong buffers) across all depth steps.  Lane q of a warp owns shot q of the group
-// (its source value S and its receiver value R packed as one float4), lanes are split into
-// 32/G position groups, and each position group sweeps blocks of X consecutive positions.  The
+// memory (ping-pong buffers) across all depth steps.  A slot holds one shot, or several shots
+// whose apertures are disjoint (uneven-aperture surveys pack into fewer slots).  Lane q of a warp
+// owns slot q (its source value S and receiver value R packed as one float4), lanes are split
+// into 32/G position groups, and each position group sweeps blocks of X consecutive positions.  The
 // operator row of a position is loaded once per lane group and broadcast to the G shots.
 // The receiver is stored conjugated in the single-table mode: conj(R_new) = sum_k T_f conj(R_old)
 // when T_b = conj(T_f), so source and receiver share every operator load.
@@ -38,6 +39,16 @@ enum OpMode : int {
     OP_DENSE = 2,  // dense tables (nextrap, nf, nx, L), reference layout
 };
 
+// A work group: up to G lane slots over a union window [u0, u0+W) of the model.  Each slot holds
+// one or more shots whose apertures are disjoint and separated by at least M zero samples, so the
+// FIR of one never reads another (the zero-halo semantics of cpp_src/wfPad.h hold per shot).
+struct GroupDesc {
+    int seg_begin, nseg;  // segments [seg_begin, seg_begin+nseg) of MigrateArgs::segs
+    int u0, W;            // union window
+    int nslots, owner_stride;
+    long long owner_off;  // start of this group's owner table
+};
+
 // Everything a migration kernel launch needs (device pointers).
 struct MigrateArgs {
     int nextrap;     // depth steps
@@ -47,9 +58,9 @@ struct MigrateArgs {
     int tab_stride;  // complex elements per compact-table row (even, >= L)
     int n_items;
     const int2 *items;       // x = group, y = frequency index, decreasing cost
-    const int4 *groups;      // x = first entry in group_shots, y = shots, z = u0, w = width
-    const int *group_shots;  // shot ids
-    const int2 *shot_win;    // x = x0, y = nx_s
+    const GroupDesc *groups;
+    const int4 *segs;        // x = shot, y = slot in its group, z = x0, w = nx_s
+    const int16_t *owner;    // per group [slot][owner_stride]: shot id at each position, -1 outside
     const long long *shot_off;  // element offset of each shot's block in wave/shot
     const cpx *tabF;
     const cpx *tabB;
@@ -80,41 +91,70 @@ __device__ __forceinline__ void kahan_add(float *s, float *c, float v)
 
 // One work item: stage the wavefields of the group for frequency j into shared memory.
 template <int G>
-__device__ __forceinline__ void stage_in(const MigrateArgs &a, float4 *buf, int4 grp, int j,
+__device__ __forceinline__ void stage_in(const MigrateArgs &a, float4 *buf, const GroupDesc &grp, int j,
                                          int Mp, int X, bool conj_rec)
 {
-    for (int qq = 0; qq < grp.y; ++qq) {
-        const int s = a.group_shots[grp.x + qq];
-        const int2 win = a.shot_win[s];
-        const cpx *ws = a.wave + a.shot_off[s] + (long long)j * win.y;
-        const cpx *rs = a.shot + a.shot_off[s] + (long long)j * win.y;
-        for (int i = threadIdx.x; i < win.y; i += blockDim.x) {
-            const int xl = win.x - grp.z + i + Mp;
+    for (int k = grp.seg_begin; k < grp.seg_begin + grp.nseg; ++k) {
+        const int4 sg = a.segs[k];
+        const cpx *ws = a.wave + a.shot_off[sg.x] + (long long)j * sg.w;
+        const cpx *rs = a.shot + a.shot_off[sg.x] + (long long)j * sg.w;
+        for (int i = threadIdx.x; i < sg.w; i += blockDim.x) {
+            const int xl = sg.z - grp.u0 + i + Mp;
             const cpx S = ws[i], R = rs[i];
-            buf[pad_slot(xl, X) * G + qq] = make_float4(S.re, S.im, R.re, conj_rec ? -R.im : R.im);
+            buf[pad_slot(xl, X) * G + sg.y] = make_float4(S.re, S.im, R.re, conj_rec ? -R.im : R.im);
         }
     }
 }
 
 template <int G>
-__device__ __forceinline__ void stage_out(const MigrateArgs &a, const float4 *buf, int4 grp,
+__device__ __forceinline__ void stage_out(const MigrateArgs &a, const float4 *buf, const GroupDesc &grp,
                                           int j, int Mp, int X, bool conj_rec)
 {
-    for (int qq = 0; qq < grp.y; ++qq) {
-        const int s = a.group_shots[grp.x + qq];
-        const int2 win = a.shot_win[s];
-        cpx *ws = a.wave + a.shot_off[s] + (long long)j * win.y;
-        cpx *rs = a.shot + a.shot_off[s] + (long long)j * win.y;
-        for (int i = threadIdx.x; i < win.y; i += blockDim.x) {
-            const int xl = win.x - grp.z + i + Mp;
-            const float4 v = buf[pad_slot(xl, X) * G + qq];
+    for (int k = grp.seg_begin; k < grp.seg_begin + grp.nseg; ++k) {
+        const int4 sg = a.segs[k];
+        cpx *ws = a.wave + a.shot_off[sg.x] + (long long)j * sg.w;
+        cpx *rs = a.shot + a.shot_off[sg.x] + (long long)j * sg.w;
+        for (int i = threadIdx.x; i < sg.w; i += blockDim.x) {
+            const int xl = sg.z - grp.u0 + i + Mp;
+            const float4 v = buf[pad_slot(xl, X) * G + sg.y];
             ws[i] = cpx{v.x, v.y};
             rs[i] = cpx{v.z, conj_rec ? -v.w : v.w};
         }
     }
 }
 
+// Shot ids of X consecutive positions of one slot (X = 4 or 8; 8- or 16-byte aligned rows).
+template <int X>
+__device__ __forceinline__ void load_owner(const int16_t *row, int16_t (&own)[X])
+{
+    if (row == nullptr) {
+#pragma unroll
+        for (int i = 0; i < X; ++i) own[i] = -1;
+        return;
+    }
+    if (X == 8) {
+        const int4 v = *reinterpret_cast<const int4 *>(row);
+        const int w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+        for (int i = 0; i < X; ++i) own[i] = (int16_t)(w[i / 2] >> (16 * (i & 1)));
+    } else {
+        const int2 v = *reinterpret_cast<const int2 *>(row);
+        const int w[2] = {v.x, v.y};
+#pragma unroll
+        for (int i = 0; i < X; ++i) own[i] = (int16_t)(w[i / 2] >> (16 * (i & 1)));
+    }
+}
+
 // Imaging + masking epilogue for one position of a block.
+// The G lanes of one position group always run the same block loop, but different position
+// groups of a warp may not (their block counts can differ by one), so the reduction over shots
+// synchronises only the group's own lanes.
+template <int G>
+__device__ __forceinline__ unsigned group_mask(int lane)
+{
+    return G == 32 ? 0xffffffffu : (((1u << G) - 1u) << ((lane / G) * G));
+}
+
 template <int G>
 __device__ __forceinline__ void emit_position(const MigrateArgs &a, float4 *dst, int slot, int q,
                                               bool in_win, bool in_group, int xm, int l, int shot_id,
@@ -128,7 +168,7 @@ __device__ __forceinline__ void emit_position(const MigrateArgs &a, float4 *dst,
     if (a.image_shots && in_win)
         atomicAdd(a.image_shots + (long long)shot_id * a.img_sstride + (long long)l * a.nx + xm, img);
 #pragma unroll
-    for (int off = 1; off < G; off <<= 1) img += __shfl_xor_sync(0xffffffffu, img, off);
+    for (int off = 1; off < G; off <<= 1) img += __shfl_xor_sync(group_mask<G>(threadIdx.x & 31), img, off);
     if (part_row && q == 0 && in_group) kahan_add(part_row + xm, comp_row + xm, img);
 }
 
@@ -160,8 +200,8 @@ __global__ void __launch_bounds__(256, 1) migrate_fixed_kernel(MigrateArgs a)
         __syncthreads();
         if (it >= a.n_items) break;
         const int2 item = a.items[it];
-        const int4 grp = a.groups[item.x];
-        const int j = item.y, u0 = grp.z, W = grp.w;
+        const GroupDesc grp = a.groups[item.x];
+        const int j = item.y, u0 = grp.u0, W = grp.W;
         const int Wp = ((W + X - 1) / X) * X;
         const int npos = Mp + Wp + Mp;
         const int nslot = npos / X * (X + 1);
@@ -171,14 +211,8 @@ __global__ void __launch_bounds__(256, 1) migrate_fixed_kernel(MigrateArgs a)
         stage_in<G>(a, bufA, grp, j, Mp, X, CONJ);
         __syncthreads();
 
-        const bool have = q < grp.y;
-        const int shot_id = have ? a.group_shots[grp.x + q] : 0;
-        int lo = 0, hi = 0;
-        if (have) {
-            const int2 win = a.shot_win[shot_id];
-            lo = win.x - u0 + Mp;
-            hi = lo + win.y;
-        }
+        const int16_t *own_base =
+            q < grp.nslots ? a.owner + grp.owner_off + (long long)q * grp.owner_stride : nullptr;
         const int nblocks = Wp / X;
         const uint16_t *idx_j = a.idx + (long long)j * a.idx_jstride;
 
@@ -231,12 +265,14 @@ __global__ void __launch_bounds__(256, 1) migrate_fixed_kernel(MigrateArgs a)
                         }
                     }
                 }
+                int16_t own[X];
+                load_owner<X>(own_base ? own_base + b * X : nullptr, own);
 #pragma unroll
                 for (int jj = 0; jj < X; ++jj) {
                     const int xl = xb + jj;
                     const int xr = b * X + jj;  // position relative to u0
-                    emit_position<G>(a, bufB, pad_slot(xl, X), q, xl >= lo && xl < hi, xr < W,
-                                     u0 + (xr < W ? xr : 0), l, shot_id, sr[jj], si[jj], rr[jj], ri[jj],
+                    emit_position<G>(a, bufB, pad_slot(xl, X), q, own[jj] >= 0, xr < W,
+                                     u0 + (xr < W ? xr : 0), l, own[jj], sr[jj], si[jj], rr[jj], ri[jj],
                                      CONJ, prow, crow);
                 }
             }
@@ -276,8 +312,8 @@ __global__ void __launch_bounds__(256, 1) migrate_generic_kernel(MigrateArgs a)
         __syncthreads();
         if (it >= a.n_items) break;
         const int2 item = a.items[it];
-        const int4 grp = a.groups[item.x];
-        const int j = item.y, u0 = grp.z, W = grp.w;
+        const GroupDesc grp = a.groups[item.x];
+        const int j = item.y, u0 = grp.u0, W = grp.W;
         const int Wp = ((W + X - 1) / X) * X;
         const int npos = Mp + Wp + Mp;
         const int nslot = npos / X * (X + 1);
@@ -287,14 +323,8 @@ __global__ void __launch_bounds__(256, 1) migrate_generic_kernel(MigrateArgs a)
         stage_in<G>(a, bufA, grp, j, Mp, X, CONJ);
         __syncthreads();
 
-        const bool have = q < grp.y;
-        const int shot_id = have ? a.group_shots[grp.x + q] : 0;
-        int lo = 0, hi = 0;
-        if (have) {
-            const int2 win = a.shot_win[shot_id];
-            lo = win.x - u0 + Mp;
-            hi = lo + win.y;
-        }
+        const int16_t *own_base =
+            q < grp.nslots ? a.owner + grp.owner_off + (long long)q * grp.owner_stride : nullptr;
         const int nblocks = Wp / X;
 
         for (int l = 0; l < a.nextrap; ++l) {
@@ -334,12 +364,14 @@ __global__ void __launch_bounds__(256, 1) migrate_generic_kernel(MigrateArgs a)
                     }
                     sr[jj] = a0; si[jj] = a1; rr[jj] = a2; ri[jj] = a3;
                 }
+                int16_t own[X];
+                load_owner<X>(own_base ? own_base + b * X : nullptr, own);
 #pragma unroll
                 for (int jj = 0; jj < X; ++jj) {
                     const int xl = xb + jj;
                     const int xr = b * X + jj;
-                    emit_position<G>(a, bufB, pad_slot(xl, X), q, xl >= lo && xl < hi, xr < W,
-                                     u0 + (xr < W ? xr : 0), l, shot_id, sr[jj], si[jj], rr[jj], ri[jj],
+                    emit_position<G>(a, bufB, pad_slot(xl, X), q, own[jj] >= 0, xr < W,
+                                     u0 + (xr < W ? xr : 0), l, own[jj], sr[jj], si[jj], rr[jj], ri[jj],
                                      CONJ, prow, crow);
                 }
             }

@@ -80,7 +80,9 @@ def _rand_dense(ns, nextrap, nz, nx, nf, nt, M, seed):
     def c(*shape):
         return (rng.standard_normal(shape) + 1j * rng.standard_normal(shape)).astype(np.complex64)
 
-    return c(nextrap, nf, nx, L) * (0.6 / np.sqrt(L)), c(nextrap, nf, nx, L) * (0.6 / np.sqrt(L)), c(ns, nt, nx), c(ns, nt, nx)
+    scale = np.float32(0.6 / np.sqrt(L))
+    return (c(nextrap, nf, nx, L) * scale).astype(np.complex64), (c(nextrap, nf, nx, L) * scale).astype(np.complex64), \
+        c(ns, nt, nx), c(ns, nt, nx)
 
 
 @pytest.mark.parametrize("ns,nextrap,nz,nx,nf,nt,M", [
