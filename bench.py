@@ -48,6 +48,7 @@ def parse_args():
     p.add_argument("--no-naive", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--accuracy", action="store_true", help="also measure rel-L2 vs the FP64 oracle on a sub-volume")
+    p.add_argument("--no-cluster", action="store_true", help="single-CTA kernels only (comparison)")
     return p.parse_args()
 
 
@@ -118,14 +119,19 @@ class ClockSampler:
 
 
 class quiet_stdout:
-    """Send file descriptor 1 to stderr while a C library that prints on stdout runs."""
+    """Send file descriptor 1 to stderr while a C library that prints on stdout runs (its stdio
+    buffer is flushed before fd 1 is restored)."""
 
     def __enter__(self):
+        import ctypes
+        self.libc = ctypes.CDLL(None)
         sys.stdout.flush()
+        self.libc.fflush(None)
         self.saved = os.dup(1)
         os.dup2(2, 1)
 
     def __exit__(self, *exc):
+        self.libc.fflush(None)
         os.dup2(self.saved, 1)
         os.close(self.saved)
 
@@ -234,7 +240,7 @@ def main():
     # weak scaling: each rank its own seeded shot set of the full per-GPU size
     maker = synthetic.WORKLOADS[args.workload]
     w = maker(seed=100 + rank, scale=args.scale) if world > 1 else maker(scale=args.scale)
-    plan = migration.Plan.for_workload(w)
+    plan = migration.Plan.for_workload(w, no_cluster=args.no_cluster)
     om = torch.from_numpy(w.omega).to(dev)
     vel = torch.from_numpy(np.ascontiguousarray(w.velocity)).to(dev)
     tab = torch.from_numpy(w.table).to(dev)

@@ -22,6 +22,7 @@ IMG2D_ECUDA = 3
 IMG2D_ENODEV = 4
 FLAG_TWO_TABLES = 1
 FLAG_GENERIC = 2
+FLAG_NO_CLUSTER = 4
 
 ERROR_NAMES = {1: "EINVAL", 2: "ENOMEM", 3: "ECUDA", 4: "ENODEV"}
 

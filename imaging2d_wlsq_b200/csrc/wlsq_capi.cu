@@ -10,6 +10,7 @@
 
 #include "../../include/imaging2d_wlsq_b200.h"
 #include "wlsq_kernels.cuh"
+#include "wlsq_cluster.cuh"
 
 namespace img2d {
 
@@ -75,6 +76,27 @@ static KernelFn find_generic(int G, int mode)
     }
     IMG2D_GEN(1) IMG2D_GEN(2) IMG2D_GEN(4) IMG2D_GEN(8)
 #undef IMG2D_GEN
+    return nullptr;
+}
+
+struct ClusterKernel {
+    int L;
+    KernelFn fn;
+    size_t smem;
+};
+
+static const ClusterKernel kCluster[] = {
+    {25, migrate_cluster_kernel<25>, cluster_smem_bytes<25>()},
+    {31, migrate_cluster_kernel<31>, cluster_smem_bytes<31>()},
+    {35, migrate_cluster_kernel<35>, cluster_smem_bytes<35>()},
+    {43, migrate_cluster_kernel<43>, cluster_smem_bytes<43>()},
+    {55, migrate_cluster_kernel<55>, cluster_smem_bytes<55>()},
+};
+
+static const ClusterKernel *find_cluster(int L)
+{
+    for (const auto &k : kCluster)
+        if (k.L == L) return &k;
     return nullptr;
 }
 
@@ -193,6 +215,7 @@ struct img2d_plan {
         if (ev1) cudaEventDestroy(ev1);
     }
     int n_slots = 0;
+    int cluster = 0;  // CTAs per cluster of the cluster kernel, 0 = single-CTA kernels
     img2d::DevBuf items, groups, segs, owner, shot_off, idx, tabF, tabB, partial, comp, counter, naive_buf;
     // dense tables (drop-in ABI) are owned by the caller of run_dense
 };
@@ -247,31 +270,16 @@ static int build_plan(img2d_plan *p, int ns, int nextrap, int nz, int nx, int nf
     }
     p->wave_elems = acc;
 
-    // Choose shots per CTA: the largest power of two <= 8 whose ping-pong buffers fit in shared
-    // memory for the widest aperture, not above the shot count rounded up to a power of two.
     int dev = 0;
     IMG2D_CUDA(cudaGetDevice(&dev));
     int smem_optin = 0, nsm = 0;
     IMG2D_CUDA(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
     IMG2D_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-    const int maxw = *std::max_element(p->w.begin(), p->w.end());
-    int nsp2 = 1;
-    while (nsp2 < ns) nsp2 <<= 1;
     const int static_reserve = 1024;
-    int G = 8;
-    while (G > 1 && (G > nsp2 || smem_bytes(G, nx, M, kX) + static_reserve > (size_t)smem_optin)) G >>= 1;
-    const bool use_fixed = (mode == OP_CONJ) && !(flags & IMG2D_FLAG_GENERIC) && find_fixed(G, p->L);
-    const int X = use_fixed ? kX : 4;
-    if (smem_bytes(G, nx, M, X) + static_reserve > (size_t)smem_optin)
-        return fail(IMG2D_EINVAL, "aperture too wide for one CTA's shared memory");
-    p->G = G;
-    p->fixed = use_fixed;
-    p->fn = use_fixed ? find_fixed(G, p->L) : find_generic(G, mode);
 
     // Pack shots into lane slots: shots sorted by aperture start go to the slot whose last shot
     // ends furthest to the left while still leaving >= M zero samples before this one (interval
-    // colouring, best fit); full-aperture shots get a slot each.  Then slots of similar extent
-    // form groups of G that share a work item.
+    // colouring, best fit); full-aperture shots get a slot each.
     std::vector<int> order(ns);
     std::iota(order.begin(), order.end(), 0);
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
@@ -299,40 +307,82 @@ static int build_plan(img2d_plan *p, int ns, int nextrap, int nz, int nx, int nf
         if (ext0(a) != ext0(b)) return ext0(a) < ext0(b);
         return slot_end[a] < slot_end[b];
     });
+    p->n_slots = (int)slots.size();
+
+    // Slots of similar extent form groups of G that share a work item.
     std::vector<GroupDesc> groups;
     std::vector<int4> segs;
     std::vector<int16_t> owner;
-    int widest = 0;
-    for (size_t g0 = 0; g0 < sorder.size(); g0 += G) {
-        const int n = (int)std::min<size_t>(G, sorder.size() - g0);
-        int u0 = nx, u1 = 0;
-        for (int k = 0; k < n; ++k) {
-            const int i = sorder[g0 + k];
-            u0 = std::min(u0, ext0(i));
-            u1 = std::max(u1, slot_end[i]);
-        }
-        GroupDesc gd{};
-        gd.seg_begin = (int)segs.size();
-        gd.u0 = u0;
-        gd.W = u1 - u0;
-        gd.nslots = n;
-        gd.owner_stride = (gd.W + 7) / 8 * 8;
-        gd.owner_off = (long long)owner.size();
-        owner.resize(owner.size() + (size_t)n * gd.owner_stride, (int16_t)-1);
-        for (int k = 0; k < n; ++k) {
-            for (int s : slots[sorder[g0 + k]]) {
-                segs.push_back(make_int4(s, k, p->x0[s], p->w[s]));
-                int16_t *row = owner.data() + gd.owner_off + (size_t)k * gd.owner_stride;
-                for (int x = p->x0[s]; x < p->x0[s] + p->w[s]; ++x) row[x - u0] = (int16_t)s;
+    auto make_groups = [&](int G) {
+        groups.clear();
+        segs.clear();
+        owner.clear();
+        int widest = 0;
+        for (size_t g0 = 0; g0 < sorder.size(); g0 += G) {
+            const int n = (int)std::min<size_t>(G, sorder.size() - g0);
+            int u0 = nx, u1 = 0;
+            for (int k = 0; k < n; ++k) {
+                const int i = sorder[g0 + k];
+                u0 = std::min(u0, ext0(i));
+                u1 = std::max(u1, slot_end[i]);
             }
+            GroupDesc gd{};
+            gd.seg_begin = (int)segs.size();
+            gd.u0 = u0;
+            gd.W = u1 - u0;
+            gd.nslots = n;
+            gd.owner_stride = (gd.W + 7) / 8 * 8;
+            gd.owner_off = (long long)owner.size();
+            owner.resize(owner.size() + (size_t)n * gd.owner_stride, (int16_t)-1);
+            for (int k = 0; k < n; ++k) {
+                for (int s : slots[sorder[g0 + k]]) {
+                    segs.push_back(make_int4(s, k, p->x0[s], p->w[s]));
+                    int16_t *row = owner.data() + gd.owner_off + (size_t)k * gd.owner_stride;
+                    for (int x = p->x0[s]; x < p->x0[s] + p->w[s]; ++x) row[x - u0] = (int16_t)s;
+                }
+            }
+            gd.nseg = (int)segs.size() - gd.seg_begin;
+            groups.push_back(gd);
+            widest = std::max(widest, gd.W);
         }
-        gd.nseg = (int)segs.size() - gd.seg_begin;
-        groups.push_back(gd);
-        widest = std::max(widest, gd.W);
+        return widest;
+    };
+
+    // Kernel choice.  The cluster kernel (16 slots per item, 256 positions per CTA, up to 8 CTAs
+    // per cluster) when the operator length has an instance, there are enough slots to fill it
+    // and the widest group fits 8 CTAs; otherwise the single-CTA kernels with the largest power
+    // of two <= 8 slots whose ping-pong buffers fit in shared memory.
+    p->cluster = 0;
+    const ClusterKernel *ck = (mode == OP_CONJ && !(flags & (IMG2D_FLAG_GENERIC | IMG2D_FLAG_NO_CLUSTER)))
+                                  ? find_cluster(p->L)
+                                  : nullptr;
+    if (ck && p->n_slots >= 12 && ck->smem + static_reserve <= (size_t)smem_optin) {
+        const int widest = make_groups(ClusterShape::G);
+        const int K = (widest + ClusterShape::PC - 1) / ClusterShape::PC;
+        if (K <= 8) {
+            p->cluster = K == 1 ? 1 : (K <= 2 ? 2 : (K <= 4 ? 4 : 8));
+            p->G = ClusterShape::G;
+            p->fixed = true;
+            p->fn = ck->fn;
+            p->smem = ck->smem;
+            p->max_w = widest;
+        }
     }
-    p->n_slots = (int)slots.size();
-    p->max_w = widest;
-    p->smem = smem_bytes(G, widest, M, X);
+    if (!p->cluster) {
+        int nsp2 = 1;
+        while (nsp2 < p->n_slots) nsp2 <<= 1;
+        int G = 8;
+        while (G > 1 && (G > nsp2 || smem_bytes(G, nx, M, kX) + static_reserve > (size_t)smem_optin)) G >>= 1;
+        const bool use_fixed = (mode == OP_CONJ) && !(flags & IMG2D_FLAG_GENERIC) && find_fixed(G, p->L);
+        const int X = use_fixed ? kX : 4;
+        if (smem_bytes(G, nx, M, X) + static_reserve > (size_t)smem_optin)
+            return fail(IMG2D_EINVAL, "aperture too wide for one CTA's shared memory");
+        p->G = G;
+        p->fixed = use_fixed;
+        p->fn = use_fixed ? find_fixed(G, p->L) : find_generic(G, mode);
+        p->max_w = make_groups(G);
+        p->smem = smem_bytes(G, p->max_w, M, X);
+    }
     // Items (group, frequency), widest groups first so the tail of the queue is short work.
     std::vector<int2> items;
     items.reserve(groups.size() * (size_t)nf);
@@ -342,7 +392,26 @@ static int build_plan(img2d_plan *p, int ns, int nextrap, int nz, int nx, int nf
     for (int g : gorder)
         for (int j = 0; j < nf; ++j) items.push_back(make_int2(g, j));
     p->n_items = (int)items.size();
-    p->grid = std::min(p->n_items, nsm);
+    IMG2D_CUDA(cudaFuncSetAttribute(p->fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->smem));
+    if (p->cluster) {
+        cudaLaunchConfig_t cfg{};
+        cudaLaunchAttribute attr{};
+        attr.id = cudaLaunchAttributeClusterDimension;
+        attr.val.clusterDim.x = p->cluster;
+        attr.val.clusterDim.y = 1;
+        attr.val.clusterDim.z = 1;
+        cfg.gridDim = dim3(p->cluster * 64, 1, 1);
+        cfg.blockDim = dim3(256, 1, 1);
+        cfg.dynamicSmemBytes = p->smem;
+        cfg.attrs = &attr;
+        cfg.numAttrs = 1;
+        int nclusters = 0;
+        IMG2D_CUDA(cudaOccupancyMaxActiveClusters(&nclusters, (void *)p->fn, &cfg));
+        if (nclusters <= 0) return fail(IMG2D_ECUDA, "no cluster of this size fits on the device");
+        p->grid = std::min(p->n_items, nclusters) * p->cluster;
+    } else {
+        p->grid = std::min(p->n_items, nsm);
+    }
 
     int rc;
     if ((rc = p->items.ensure(items.size() * sizeof(int2)))) return rc;
@@ -356,7 +425,6 @@ static int build_plan(img2d_plan *p, int ns, int nextrap, int nz, int nx, int nf
     IMG2D_CUDA(cudaMemcpy(p->segs.p, segs.data(), segs.size() * sizeof(int4), cudaMemcpyHostToDevice));
     IMG2D_CUDA(cudaMemcpy(p->owner.p, owner.data(), owner.size() * sizeof(int16_t), cudaMemcpyHostToDevice));
     IMG2D_CUDA(cudaMemcpy(p->shot_off.p, p->off.data(), p->off.size() * sizeof(long long), cudaMemcpyHostToDevice));
-    IMG2D_CUDA(cudaFuncSetAttribute(p->fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->smem));
     const size_t plane = (size_t)nextrap * nx;
     if ((rc = p->partial.ensure((size_t)p->grid * plane * sizeof(float)))) return rc;
     if ((rc = p->comp.ensure((size_t)p->grid * plane * sizeof(float)))) return rc;
@@ -419,7 +487,23 @@ static int launch(img2d_plan *p, MigrateArgs a, float *d_image, float *d_image_s
         IMG2D_CUDA(cudaEventCreate(&p->ev1));
     }
     IMG2D_CUDA(cudaEventRecord(p->ev0, st));
-    p->fn<<<p->grid, 256, p->smem, st>>>(a);
+    if (p->cluster) {
+        cudaLaunchConfig_t cfg{};
+        cudaLaunchAttribute attr{};
+        attr.id = cudaLaunchAttributeClusterDimension;
+        attr.val.clusterDim.x = p->cluster;
+        attr.val.clusterDim.y = 1;
+        attr.val.clusterDim.z = 1;
+        cfg.gridDim = dim3(p->grid, 1, 1);
+        cfg.blockDim = dim3(256, 1, 1);
+        cfg.dynamicSmemBytes = p->smem;
+        cfg.stream = st;
+        cfg.attrs = &attr;
+        cfg.numAttrs = 1;
+        IMG2D_CUDA(cudaLaunchKernelEx(&cfg, p->fn, a));
+    } else {
+        p->fn<<<p->grid, 256, p->smem, st>>>(a);
+    }
     IMG2D_CUDA(cudaGetLastError());
     IMG2D_CUDA(cudaEventRecord(p->ev1, st));
     p->ev_recorded = true;
@@ -603,9 +687,10 @@ int img2d_plan_describe(const img2d_plan *p, char *buf, int buflen)
 {
     if (!p || !buf || buflen <= 0) return fail(IMG2D_EINVAL, "bad describe arguments");
     snprintf(buf, buflen,
-             "{\"kernel\": \"%s\", \"G\": %d, \"X\": %d, \"L\": %d, \"grid\": %d, \"block\": 256, "
+             "{\"kernel\": \"%s\", \"cluster\": %d, \"G\": %d, \"X\": %d, \"L\": %d, \"grid\": %d, \"block\": 256, "
              "\"smem\": %zu, \"items\": %d, \"slots\": %d, \"max_union_width\": %d, \"mode\": %d}",
-             p->fixed ? "migrate_fixed" : "migrate_generic", p->G, p->fixed ? kX : 4, p->L, p->grid, p->smem,
+             p->cluster ? "migrate_cluster" : (p->fixed ? "migrate_fixed" : "migrate_generic"), p->cluster, p->G,
+             p->fixed ? kX : 4, p->L, p->grid, p->smem,
              p->n_items, p->n_slots, p->max_w, p->mode);
     return IMG2D_OK;
 }

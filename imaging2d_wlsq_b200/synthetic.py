@@ -140,20 +140,22 @@ def plain_small(seed=1, scale=1.0, tables=True):
     return _finish(w, 2.0, 30.0, 15.0, rng, tables)
 
 
-def plain_medium(seed=2, scale=1.0, tables=True, ns=32):
-    nz, nx = max(8, int(500 * scale)), max(32, int(1024 * scale))
+def plain_medium(seed=2, scale=1.0, tables=True, ns=32, nz=None, nx=None, nf=None):
+    nz = nz or max(8, int(500 * scale))
+    nx = nx or max(32, int(1024 * scale))
     rng = np.random.default_rng(seed)
     v = gaussian_random_field(nz, nx, 50.0 * max(scale, 0.1), 1500.0, 4500.0, rng)
     ns = max(1, int(ns * min(1.0, scale * 4))) if scale < 1.0 else ns
     pos = np.linspace(nx / (2 * ns), nx - nx / (2 * ns), ns).astype(np.int32)
     x0, wdt, pos = _full_aperture(ns, nx, pos)
-    w = Workload("plain_medium", nz, nx, 10.0, 10.0, max(4, int(256 * scale)), 15, max(64, int(2000 * scale)), 0.0,
-                 None, v, None, x0, wdt, pos, nextrap=nz, seed=seed)
+    w = Workload("plain_medium", nz, nx, 10.0, 10.0, nf or max(4, int(256 * scale)), 15,
+                 max(64, int(2000 * scale)), 0.0, None, v, None, x0, wdt, pos, nextrap=nz, seed=seed)
     return _finish(w, 2.0, 40.0, 20.0, rng, tables)
 
 
-def batched_uneven(seed=3, scale=1.0, tables=True, ns=256):
-    nz, nx = max(8, int(1000 * scale)), max(64, int(2048 * scale))
+def batched_uneven(seed=3, scale=1.0, tables=True, ns=256, nz=None, nx=None, nf=None):
+    nz = nz or max(8, int(1000 * scale))
+    nx = nx or max(64, int(2048 * scale))
     rng = np.random.default_rng(seed)
     v = gaussian_random_field(nz, nx, 50.0 * max(scale, 0.1), 1500.0, 4500.0, rng)
     ns = max(2, int(ns * scale)) if scale < 1.0 else ns
@@ -167,8 +169,8 @@ def batched_uneven(seed=3, scale=1.0, tables=True, ns=256):
     x1[bad] = x0[bad] + 2
     wdt = (x1 - x0).astype(np.int32)
     pos = np.clip(centre, x0, x1 - 1).astype(np.int32)
-    w = Workload("batched_uneven", nz, nx, 10.0, 10.0, max(4, int(512 * scale)), 17, max(64, int(4000 * scale)), 0.0,
-                 None, v, None, x0, wdt, pos, nextrap=nz, seed=seed)
+    w = Workload("batched_uneven", nz, nx, 10.0, 10.0, nf or max(4, int(512 * scale)), 17,
+                 max(64, int(4000 * scale)), 0.0, None, v, None, x0, wdt, pos, nextrap=nz, seed=seed)
     return _finish(w, 2.0, 50.0, 20.0, rng, tables)
 
 

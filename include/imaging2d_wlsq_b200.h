@@ -36,6 +36,7 @@ typedef struct {
 /* flags for the compact-table entry points */
 #define IMG2D_FLAG_TWO_TABLES 1   /* use tab_back for the receiver instead of conj(tab_forw) */
 #define IMG2D_FLAG_GENERIC 2      /* force the runtime-length kernel (testing) */
+#define IMG2D_FLAG_NO_CLUSTER 4   /* use the single-CTA kernels even where the cluster kernel applies */
 
 const char *img2d_last_error(void);
 int img2d_version(void);

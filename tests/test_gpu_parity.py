@@ -211,3 +211,27 @@ def test_invalid_arguments_raise():
                        shot_nx=[w.nx] * 4)
     with pytest.raises(LibraryError):
         migration.Plan(w.ns, w.nz + 1, w.nz, w.nx, w.nf, w.nt, w.M, w.nk)
+
+
+@pytest.mark.parametrize("kind,nx,nz,nf,ns", [("medium", 256, 12, 6, 16), ("medium", 480, 10, 5, 24),
+                                              ("uneven", 1000, 8, 5, 40), ("uneven", 2048, 6, 4, 64),
+                                              ("medium", 2048, 5, 3, 32)])
+def test_cluster_kernel_matches_oracle_and_single_cta(kind, nx, nz, nf, ns):
+    """Clusters of 1, 2, 4 and 8 CTAs (256 positions each) against the FP64 oracle and against the
+    single-CTA kernel; few depth steps and frequencies keep the oracle fast."""
+    if kind == "medium":
+        w = synthetic.plain_medium(nx=nx, nz=nz, nf=nf, ns=ns, scale=1.0)
+    else:
+        w = synthetic.batched_uneven(nx=nx, nz=nz, nf=nf, ns=ns, scale=1.0)
+    plan = migration.Plan.for_workload(w)
+    d = plan.describe()
+    plan.close()
+    assert d["kernel"] == "migrate_cluster", d
+    assert d["cluster"] == {256: 1, 480: 2, 1000: 4, 2048: 8}[nx] or kind == "uneven", d
+    img, imgs, wave, shot = migration.migrate_workload(w, image_shots=True)
+    e = _compact_check(w, img, wave, shot)
+    img1, _, wave1, _ = migration.migrate_workload(w, no_cluster=True)
+    assert rel_l2(img, img1) <= 2e-6 and rel_l2(wave, wave1) <= 2e-6
+    _, shots_o, _, _ = oracle.migrate_workload_f64(w)
+    assert rel_l2(imgs, shots_o) <= 1e-5
+    assert e <= 1e-5
