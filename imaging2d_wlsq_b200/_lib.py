@@ -23,6 +23,7 @@ IMG2D_ENODEV = 4
 FLAG_TWO_TABLES = 1
 FLAG_GENERIC = 2
 FLAG_NO_CLUSTER = 4
+NOALLOC_SCRATCH_BYTES = 64 << 20
 
 ERROR_NAMES = {1: "EINVAL", 2: "ENOMEM", 3: "ECUDA", 4: "ENODEV"}
 
@@ -85,6 +86,8 @@ def load():
     lib.img2d_plan_kernel_ms.argtypes = [c_void_p, POINTER(ctypes.c_float)]
     lib.img2d_measure_fp32_peak.restype = c_int
     lib.img2d_measure_fp32_peak.argtypes = [POINTER(c_double)]
+    lib.img2d_migrate_compact_noalloc.restype = c_int
+    lib.img2d_migrate_compact_noalloc.argtypes = [c_int] * 8 + [c_double] + [c_void_p] * 9
     lib.img2d_plan_destroy.restype = None
     lib.img2d_plan_destroy.argtypes = [c_void_p]
     return lib

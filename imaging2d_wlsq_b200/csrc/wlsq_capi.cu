@@ -168,20 +168,40 @@ __global__ void fma_probe_kernel(float *out, int iters)
 // ---------------------------------------------------------------------------------------
 // Plan
 // ---------------------------------------------------------------------------------------
+// Bump allocator over a fixed device region (the no-allocation entry point's static scratch).
+struct Carver {
+    unsigned char *base = nullptr;
+    size_t cap = 0, used = 0;
+};
+
 struct DevBuf {
     void *p = nullptr;
     size_t bytes = 0;
+    bool owned = false;
+    Carver *carver = nullptr;  // when set, storage is carved from it and never freed
     ~DevBuf() { release(); }
     void release()
     {
-        if (p) cudaFree(p);
+        if (p && owned) cudaFree(p);
         p = nullptr;
         bytes = 0;
+        owned = false;
     }
     int ensure(size_t n)
     {
         if (n <= bytes && p) return IMG2D_OK;
         release();
+        if (carver) {
+            const size_t off = (carver->used + 255) & ~(size_t)255;
+            if (off + n > carver->cap)
+                return fail(IMG2D_EINVAL, "problem needs more than the " + std::to_string(carver->cap >> 20) +
+                                              " MiB of fixed scratch of the no-allocation entry point");
+            p = carver->base + off;
+            bytes = n;
+            carver->used = off + n;
+            return IMG2D_OK;
+        }
+        owned = true;
         if (n == 0) n = 16;
         cudaError_t e = cudaMalloc(&p, n);
         if (e != cudaSuccess) {
@@ -216,6 +236,9 @@ struct img2d_plan {
     }
     int n_slots = 0;
     int cluster = 0;  // CTAs per cluster of the cluster kernel, 0 = single-CTA kernels
+    img2d::Carver *carver = nullptr;  // no-allocation mode: buffers carved from fixed scratch
+    cudaStream_t upload_stream = 0;   // no-allocation mode: stream of the descriptor uploads
+    bool timing = true;               // record events around the migration kernel
     img2d::DevBuf items, groups, segs, owner, shot_off, idx, tabF, tabB, partial, comp, counter, naive_buf;
     // dense tables (drop-in ABI) are owned by the caller of run_dense
 };
@@ -420,12 +443,36 @@ static int build_plan(img2d_plan *p, int ns, int nextrap, int nz, int nx, int nf
     if ((rc = p->owner.ensure(owner.size() * sizeof(int16_t)))) return rc;
     if ((rc = p->shot_off.ensure(p->off.size() * sizeof(long long)))) return rc;
     if ((rc = p->counter.ensure(sizeof(int)))) return rc;
-    IMG2D_CUDA(cudaMemcpy(p->items.p, items.data(), items.size() * sizeof(int2), cudaMemcpyHostToDevice));
-    IMG2D_CUDA(cudaMemcpy(p->groups.p, groups.data(), groups.size() * sizeof(GroupDesc), cudaMemcpyHostToDevice));
-    IMG2D_CUDA(cudaMemcpy(p->segs.p, segs.data(), segs.size() * sizeof(int4), cudaMemcpyHostToDevice));
-    IMG2D_CUDA(cudaMemcpy(p->owner.p, owner.data(), owner.size() * sizeof(int16_t), cudaMemcpyHostToDevice));
-    IMG2D_CUDA(cudaMemcpy(p->shot_off.p, p->off.data(), p->off.size() * sizeof(long long), cudaMemcpyHostToDevice));
+    if (p->carver) {
+        // ordered on the caller's stream after any earlier call that used the same scratch
+        cudaStream_t us = p->upload_stream;
+        IMG2D_CUDA(cudaMemcpyAsync(p->items.p, items.data(), items.size() * sizeof(int2), cudaMemcpyHostToDevice, us));
+        IMG2D_CUDA(cudaMemcpyAsync(p->groups.p, groups.data(), groups.size() * sizeof(GroupDesc), cudaMemcpyHostToDevice, us));
+        IMG2D_CUDA(cudaMemcpyAsync(p->segs.p, segs.data(), segs.size() * sizeof(int4), cudaMemcpyHostToDevice, us));
+        IMG2D_CUDA(cudaMemcpyAsync(p->owner.p, owner.data(), owner.size() * sizeof(int16_t), cudaMemcpyHostToDevice, us));
+        IMG2D_CUDA(cudaMemcpyAsync(p->shot_off.p, p->off.data(), p->off.size() * sizeof(long long), cudaMemcpyHostToDevice, us));
+        // pageable sources: make sure the copies have read the host vectors before they go away
+        IMG2D_CUDA(cudaStreamSynchronize(us));
+    } else {
+        IMG2D_CUDA(cudaMemcpy(p->items.p, items.data(), items.size() * sizeof(int2), cudaMemcpyHostToDevice));
+        IMG2D_CUDA(cudaMemcpy(p->groups.p, groups.data(), groups.size() * sizeof(GroupDesc), cudaMemcpyHostToDevice));
+        IMG2D_CUDA(cudaMemcpy(p->segs.p, segs.data(), segs.size() * sizeof(int4), cudaMemcpyHostToDevice));
+        IMG2D_CUDA(cudaMemcpy(p->owner.p, owner.data(), owner.size() * sizeof(int16_t), cudaMemcpyHostToDevice));
+        IMG2D_CUDA(cudaMemcpy(p->shot_off.p, p->off.data(), p->off.size() * sizeof(long long), cudaMemcpyHostToDevice));
+    }
     const size_t plane = (size_t)nextrap * nx;
+    if (p->carver) {
+        // fixed scratch: fewer persistent CTAs when their private image partials would not fit
+        const size_t idx_b = (size_t)nf * nextrap * ((nx + 7) / 8 * 8) * sizeof(uint16_t) + 256;
+        const size_t tab_b = ((size_t)nk * ((p->L + 1) / 2 * 2) * sizeof(cpx) + 256) * (mode == OP_TWO ? 2 : 1);
+        const size_t used = (p->carver->used + 255) & ~(size_t)255;
+        const size_t left = p->carver->cap > used + idx_b + tab_b ? p->carver->cap - used - idx_b - tab_b : 0;
+        const size_t fit = left / (2 * plane * sizeof(float) + 512);
+        if (fit < 1)
+            return fail(IMG2D_EINVAL, "problem needs more than the " + std::to_string(p->carver->cap >> 20) +
+                                          " MiB of fixed scratch of the no-allocation entry point");
+        p->grid = (int)std::min<size_t>((size_t)p->grid, fit);
+    }
     if ((rc = p->partial.ensure((size_t)p->grid * plane * sizeof(float)))) return rc;
     if ((rc = p->comp.ensure((size_t)p->grid * plane * sizeof(float)))) return rc;
     if (mode != OP_DENSE) {
@@ -482,11 +529,11 @@ static int launch(img2d_plan *p, MigrateArgs a, float *d_image, float *d_image_s
         a.image_shots = d_image_shots;
         a.img_sstride = img_sstride;
     }
-    if (!p->ev0) {
+    if (p->timing && !p->ev0) {
         IMG2D_CUDA(cudaEventCreate(&p->ev0));
         IMG2D_CUDA(cudaEventCreate(&p->ev1));
     }
-    IMG2D_CUDA(cudaEventRecord(p->ev0, st));
+    if (p->timing) IMG2D_CUDA(cudaEventRecord(p->ev0, st));
     if (p->cluster) {
         cudaLaunchConfig_t cfg{};
         cudaLaunchAttribute attr{};
@@ -505,8 +552,10 @@ static int launch(img2d_plan *p, MigrateArgs a, float *d_image, float *d_image_s
         p->fn<<<p->grid, 256, p->smem, st>>>(a);
     }
     IMG2D_CUDA(cudaGetLastError());
-    IMG2D_CUDA(cudaEventRecord(p->ev1, st));
-    p->ev_recorded = true;
+    if (p->timing) {
+        IMG2D_CUDA(cudaEventRecord(p->ev1, st));
+        p->ev_recorded = true;
+    }
     if (d_image) {
         const int blocks = (int)std::min<size_t>((plane + 255) / 256, 148 * 8);
         reduce_partials_kernel<<<blocks, 256, 0, st>>>(p->partial.as<float>(), p->comp.as<float>(), p->grid,
@@ -605,6 +654,36 @@ static int run_dense(int ns, int nextrap, int nz, int nx, int nf, int nt, int M,
 static std::mutex g_cache_mu;
 static img2d_plan *g_cached = nullptr;
 static std::vector<int> g_cached_key;
+
+}  // namespace img2d
+
+// ---------------------------------------------------------------------------------------
+// Fixed scratch for img2d_migrate_compact_noalloc.  A file-scope device array: every GPU that
+// loads this library holds it (IMG2D_NOALLOC_SCRATCH_BYTES) until the process exits.  In host code
+// the name g_noalloc_scratch is only a stand-in for the symbol, not a device address, so the
+// address is looked up once per device with cudaGetSymbolAddress while that device is current.
+// ---------------------------------------------------------------------------------------
+static __device__ __align__(256) unsigned char g_noalloc_scratch[IMG2D_NOALLOC_SCRATCH_BYTES];
+
+namespace img2d {
+
+static std::mutex g_noalloc_mu;
+static void *g_noalloc_addr[256];
+
+static int noalloc_scratch(void **out)
+{
+    int dev = 0;
+    IMG2D_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 256) return fail(IMG2D_EINVAL, "device ordinal out of range");
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_addr[dev]) {
+        void *addr = nullptr;
+        IMG2D_CUDA(cudaGetSymbolAddress(&addr, g_noalloc_scratch));
+        g_noalloc_addr[dev] = addr;
+    }
+    *out = g_noalloc_addr[dev];
+    return IMG2D_OK;
+}
 
 }  // namespace img2d
 
@@ -778,6 +857,35 @@ int img2d_plan_execute_naive(img2d_plan *p, img2d_c64 *d_wave, img2d_c64 *d_shot
     }
     IMG2D_CUDA(cudaGetLastError());
     return IMG2D_OK;
+}
+
+int img2d_migrate_compact_noalloc(int ns, int nextrap, int nz, int nx, int nf, int nt, int M, int nk, double dk,
+                                  const double *d_omega, const double *d_velocity, const img2d_c64 *d_tab_forw,
+                                  const int *shot_x0, const int *shot_nx, img2d_c64 *d_wave, img2d_c64 *d_shot,
+                                  float *d_image, void *stream)
+{
+    int rc;
+    if ((rc = check_device())) return rc;
+    if (!d_omega || !d_velocity || !d_tab_forw || !d_wave || !d_shot || !d_image)
+        return fail(IMG2D_EINVAL, "null pointer argument");
+    void *base = nullptr;
+    if ((rc = noalloc_scratch(&base))) return rc;
+    Carver carver;
+    carver.base = static_cast<unsigned char *>(base);
+    carver.cap = IMG2D_NOALLOC_SCRATCH_BYTES;
+    img2d_plan plan;
+    plan.carver = &carver;
+    plan.upload_stream = (cudaStream_t)stream;
+    plan.timing = false;
+    for (DevBuf *b : {&plan.items, &plan.groups, &plan.segs, &plan.owner, &plan.shot_off, &plan.idx, &plan.tabF,
+                      &plan.tabB, &plan.partial, &plan.comp, &plan.counter, &plan.naive_buf})
+        b->carver = &carver;
+    if ((rc = build_plan(&plan, ns, nextrap, nz, nx, nf, nt, M, nk, shot_x0, shot_nx, IMG2D_FLAG_NO_CLUSTER, OP_CONJ)))
+        return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    if ((rc = set_model(&plan, d_omega, d_velocity, dk, (const cpx *)d_tab_forw, nullptr, st))) return rc;
+    MigrateArgs a = base_args(&plan, (cpx *)d_wave, (cpx *)d_shot);
+    return launch(&plan, a, d_image, nullptr, 0, st);
 }
 
 int img2d_migrate_compact(int ns, int nextrap, int nz, int nx, int nf, int nt, int M, int nk, double dk,

@@ -118,6 +118,33 @@ int img2d_plan_kernel_ms(img2d_plan *plan, float *ms);
  * FMA chains (the denominator of the FP32 roofline; not part of the migration path). */
 int img2d_measure_fp32_peak(double *tflops);
 
+/* ------------------------------------------------------------------------------------------
+ * No-allocation entry point.  No counterpart in the reference: the reference libraries allocate
+ * their device memory inside every call.
+ *
+ * For callers that cannot call cudaMalloc: a plugin inside a host application that owns all
+ * device memory through its own pool and forbids direct allocation, or a processing loop that
+ * must not block on (cudaMalloc can synchronise the device) or fail in an allocation mid-run.
+ * Same migration as img2d_plan_execute (single-table mode), with device pointers for every input
+ * and output; shot_x0/shot_nx are host arrays (or NULL for full aperture).  Its scratch (operator
+ * index table, padded table, work descriptors, per-CTA image partials) lives in one fixed device
+ * array of IMG2D_NOALLOC_SCRATCH_BYTES inside the library, which every GPU that loads the library
+ * holds until the process exits.  Problems whose scratch does not fit are rejected with
+ * IMG2D_EINVAL and a message naming the limit; nothing is allocated.
+ *  - The first call on a device looks up the array's device address (cudaGetSymbolAddress);
+ *    make that first call before any stream capture.
+ *  - All calls share the one array and it keeps the last call's contents (the entry point
+ *    clears what must start at zero).  Calls that overlap on the GPU race: issue them on one
+ *    stream, or wait for the previous call before the next.
+ *  - Asynchronous on `stream` except for a short upload of the work descriptors, after which the
+ *    call waits for that stream.
+ * ---------------------------------------------------------------------------------------- */
+#define IMG2D_NOALLOC_SCRATCH_BYTES (64ull << 20)
+int img2d_migrate_compact_noalloc(int ns, int nextrap, int nz, int nx, int nf, int nt, int M, int nk,
+                                  double dk, const double *d_omega, const double *d_velocity,
+                                  const img2d_c64 *d_tab_forw, const int *shot_x0, const int *shot_nx,
+                                  img2d_c64 *d_wave, img2d_c64 *d_shot, float *d_image, void *stream);
+
 /* Naive comparison form: one kernel launch per (shot, frequency, depth), operators from the
  * compact table, wavefields in global memory.  Same arguments and results as
  * img2d_plan_execute (device pointers).  Used only to measure the batched kernel against. */
