@@ -43,12 +43,16 @@ def parse_args():
     p.add_argument("--workload", default="batched_uneven")
     p.add_argument("--scale", type=float, default=1.0)
     p.add_argument("--e2e-steps", type=int, default=2)
+    p.add_argument("--variant", type=int, default=0, help="cluster-kernel variant (1-based; 0 = default)")
+    p.add_argument("--nz", type=int, default=None, help="override depth steps (profiling a reduced case)")
+    p.add_argument("--nf", type=int, default=None, help="override frequency count (profiling a reduced case)")
     p.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU-baseline sample time")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-naive", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--accuracy", action="store_true", help="also measure rel-L2 vs the FP64 oracle on a sub-volume")
-    p.add_argument("--no-cluster", action="store_true", help="single-CTA kernels only (comparison)")
+    p.add_argument("--kernel", default="auto", choices=["auto", "cluster1", "single"],
+                   help="kernel family (comparison runs); auto = the plan's choice")
     return p.parse_args()
 
 
@@ -239,8 +243,10 @@ def main():
 
     # weak scaling: each rank its own seeded shot set of the full per-GPU size
     maker = synthetic.WORKLOADS[args.workload]
-    w = maker(seed=100 + rank, scale=args.scale) if world > 1 else maker(scale=args.scale)
-    plan = migration.Plan.for_workload(w, no_cluster=args.no_cluster)
+    over = {k: v for k, v in (("nz", args.nz), ("nf", args.nf)) if v}
+    w = maker(seed=100 + rank, scale=args.scale, **over) if world > 1 else maker(scale=args.scale, **over)
+    plan = migration.Plan.for_workload(w, no_cluster=args.kernel == "single", cluster_v1=args.kernel == "cluster1",
+                                       variant=args.variant)
     om = torch.from_numpy(w.omega).to(dev)
     vel = torch.from_numpy(np.ascontiguousarray(w.velocity)).to(dev)
     tab = torch.from_numpy(w.table).to(dev)

@@ -23,6 +23,8 @@ IMG2D_ENODEV = 4
 FLAG_TWO_TABLES = 1
 FLAG_GENERIC = 2
 FLAG_NO_CLUSTER = 4
+FLAG_CLUSTER_V1 = 8
+FLAG_VARIANT_SHIFT = 8
 NOALLOC_SCRATCH_BYTES = 64 << 20
 
 ERROR_NAMES = {1: "EINVAL", 2: "ENOMEM", 3: "ECUDA", 4: "ENODEV"}

@@ -11,6 +11,7 @@
 #include "../../include/imaging2d_wlsq_b200.h"
 #include "wlsq_kernels.cuh"
 #include "wlsq_cluster.cuh"
+#include "wlsq_cluster2.cuh"
 
 namespace img2d {
 
@@ -92,6 +93,26 @@ static const ClusterKernel kCluster[] = {
     {43, migrate_cluster_kernel<43>, cluster_smem_bytes<43>()},
     {55, migrate_cluster_kernel<55>, cluster_smem_bytes<55>()},
 };
+
+// Variants of the second-generation cluster kernel: warps per CTA (positions per CTA = 32 * warps),
+// operator-pair prefetch into registers, next-step operator rows prefetched into L1.
+struct Cluster2Variant {
+    int nw;
+    bool tap_pf, row_pf;
+    KernelFn fn;
+};
+
+static const Cluster2Variant kCluster2[] = {
+    {16, false, false, migrate_cluster2_kernel<16, false, false>},
+    {16, false, true, migrate_cluster2_kernel<16, false, true>},
+    {12, true, false, migrate_cluster2_kernel<12, true, false>},
+    {12, true, true, migrate_cluster2_kernel<12, true, true>},
+    {8, true, false, migrate_cluster2_kernel<8, true, false>},
+    {8, true, true, migrate_cluster2_kernel<8, true, true>},
+    {16, false, false, migrate_cluster2_kernel<16, false, false, true>},  // packed FFMA2 arithmetic
+};
+constexpr int kCluster2Default = 0;
+constexpr int kNumCluster2 = (int)(sizeof(kCluster2) / sizeof(kCluster2[0]));
 
 static const ClusterKernel *find_cluster(int L)
 {
@@ -236,6 +257,9 @@ struct img2d_plan {
     }
     int n_slots = 0;
     int cluster = 0;  // CTAs per cluster of the cluster kernel, 0 = single-CTA kernels
+    int block = 256;                  // threads per CTA of the chosen kernel
+    int variant = -1;                 // index into the cluster2 variant table
+    const char *kname = "";           // name of the chosen kernel
     img2d::Carver *carver = nullptr;  // no-allocation mode: buffers carved from fixed scratch
     cudaStream_t upload_stream = 0;   // no-allocation mode: stream of the descriptor uploads
     bool timing = true;               // record events around the migration kernel
@@ -376,10 +400,31 @@ static int build_plan(img2d_plan *p, int ns, int nextrap, int nz, int nx, int nf
     // and the widest group fits 8 CTAs; otherwise the single-CTA kernels with the largest power
     // of two <= 8 slots whose ping-pong buffers fit in shared memory.
     p->cluster = 0;
-    const ClusterKernel *ck = (mode == OP_CONJ && !(flags & (IMG2D_FLAG_GENERIC | IMG2D_FLAG_NO_CLUSTER)))
-                                  ? find_cluster(p->L)
-                                  : nullptr;
-    if (ck && p->n_slots >= 12 && ck->smem + static_reserve <= (size_t)smem_optin) {
+    p->block = 256;
+    const bool cluster_ok = mode == OP_CONJ && !(flags & (IMG2D_FLAG_GENERIC | IMG2D_FLAG_NO_CLUSTER)) &&
+                            p->n_slots >= 12;
+    int vsel = (flags >> IMG2D_FLAG_VARIANT_SHIFT) & 0xff;
+    vsel = (vsel >= 1 && vsel <= kNumCluster2) ? vsel - 1 : kCluster2Default;
+    const Cluster2Variant &cv = kCluster2[vsel];
+    const int pc2 = cv.nw * 32;
+    if (cluster_ok && !(flags & IMG2D_FLAG_CLUSTER_V1) && p->L >= 7 &&
+        cluster2_smem_bytes(M, pc2) + static_reserve <= (size_t)smem_optin) {
+        const int widest = make_groups(16);
+        const int K = (widest + pc2 - 1) / pc2;
+        if (K <= 8) {
+            p->cluster = K;
+            p->G = 16;
+            p->fixed = true;
+            p->fn = cv.fn;
+            p->smem = cluster2_smem_bytes(M, pc2);
+            p->max_w = widest;
+            p->block = pc2;
+            p->variant = vsel;
+            p->kname = "migrate_cluster2";
+        }
+    }
+    const ClusterKernel *ck = cluster_ok ? find_cluster(p->L) : nullptr;
+    if (!p->cluster && ck && ck->smem + static_reserve <= (size_t)smem_optin) {
         const int widest = make_groups(ClusterShape::G);
         const int K = (widest + ClusterShape::PC - 1) / ClusterShape::PC;
         if (K <= 8) {
@@ -389,6 +434,7 @@ static int build_plan(img2d_plan *p, int ns, int nextrap, int nz, int nx, int nf
             p->fn = ck->fn;
             p->smem = ck->smem;
             p->max_w = widest;
+            p->kname = "migrate_cluster";
         }
     }
     if (!p->cluster) {
@@ -405,6 +451,7 @@ static int build_plan(img2d_plan *p, int ns, int nextrap, int nz, int nx, int nf
         p->fn = use_fixed ? find_fixed(G, p->L) : find_generic(G, mode);
         p->max_w = make_groups(G);
         p->smem = smem_bytes(G, p->max_w, M, X);
+        p->kname = use_fixed ? "migrate_fixed" : "migrate_generic";
     }
     // Items (group, frequency), widest groups first so the tail of the queue is short work.
     std::vector<int2> items;
@@ -424,7 +471,7 @@ static int build_plan(img2d_plan *p, int ns, int nextrap, int nz, int nx, int nf
         attr.val.clusterDim.y = 1;
         attr.val.clusterDim.z = 1;
         cfg.gridDim = dim3(p->cluster * 64, 1, 1);
-        cfg.blockDim = dim3(256, 1, 1);
+        cfg.blockDim = dim3(p->block, 1, 1);
         cfg.dynamicSmemBytes = p->smem;
         cfg.attrs = &attr;
         cfg.numAttrs = 1;
@@ -542,7 +589,7 @@ static int launch(img2d_plan *p, MigrateArgs a, float *d_image, float *d_image_s
         attr.val.clusterDim.y = 1;
         attr.val.clusterDim.z = 1;
         cfg.gridDim = dim3(p->grid, 1, 1);
-        cfg.blockDim = dim3(256, 1, 1);
+        cfg.blockDim = dim3(p->block, 1, 1);
         cfg.dynamicSmemBytes = p->smem;
         cfg.stream = st;
         cfg.attrs = &attr;
@@ -766,11 +813,10 @@ int img2d_plan_describe(const img2d_plan *p, char *buf, int buflen)
 {
     if (!p || !buf || buflen <= 0) return fail(IMG2D_EINVAL, "bad describe arguments");
     snprintf(buf, buflen,
-             "{\"kernel\": \"%s\", \"cluster\": %d, \"G\": %d, \"X\": %d, \"L\": %d, \"grid\": %d, \"block\": 256, "
-             "\"smem\": %zu, \"items\": %d, \"slots\": %d, \"max_union_width\": %d, \"mode\": %d}",
-             p->cluster ? "migrate_cluster" : (p->fixed ? "migrate_fixed" : "migrate_generic"), p->cluster, p->G,
-             p->fixed ? kX : 4, p->L, p->grid, p->smem,
-             p->n_items, p->n_slots, p->max_w, p->mode);
+             "{\"kernel\": \"%s\", \"cluster\": %d, \"G\": %d, \"X\": %d, \"L\": %d, \"grid\": %d, \"block\": %d, "
+             "\"smem\": %zu, \"items\": %d, \"slots\": %d, \"max_union_width\": %d, \"mode\": %d, \"variant\": %d}",
+             p->kname, p->cluster, p->G, p->fixed ? kX : 4, p->L, p->grid, p->block, p->smem,
+             p->n_items, p->n_slots, p->max_w, p->mode, p->variant);
     return IMG2D_OK;
 }
 

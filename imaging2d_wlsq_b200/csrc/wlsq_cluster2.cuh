@@ -1,0 +1,376 @@
+// Second-generation cluster kernel: same decomposition and results as migrate_cluster_kernel
+// (wlsq_cluster.cuh), reshaped for latency hiding on B200:
+//   * 512 threads (16 warps, 4 per scheduler) at <= 128 registers, one CTA per SM, each CTA owning
+//     512 consecutive positions of the item's window (one X=8 block per lane group), so a
+//     2048-wide window needs a cluster of 4 CTAs (clusters of 4 pack the GPCs better than 8);
+//   * the tap loop is a compact runtime loop over tap pairs with a short static prologue and
+//     epilogue, which keeps the loop body in the instruction cache and serves every odd operator
+//     length L >= 7 with one instance;
+//   * the Kahan partial-image rows of the next depth step are prefetched into L1 while the
+//     current step computes, so the imaging read-modify-write does not wait on DRAM.
+//
+// Tap loop (input-stationary): input position t (0 <= t < X+L-1, relative to block start - M)
+// contributes to output jj with tap k = t - jj when 0 <= k < L.  Taps are loaded in pairs (k, k+1)
+// as one float4 when k is even; output jj keeps its current pair in tp[jj].  For t in
+// [X-1, L-1] every jj is active; that middle range has an even number of steps (L odd, X even) and
+// runs as a loop of two steps: at the odd step the odd jj load a new pair, at the even step the
+// even jj do, and every jj uses the other half of the pair it holds.
+#pragma once
+#include "wlsq_cluster.cuh"
+
+namespace img2d {
+
+template <int NWARPS>
+struct Cluster2Shape {
+    static constexpr int Q = 8;            // lanes per position group
+    static constexpr int G = 2 * Q;        // lane slots per item (two per lane)
+    static constexpr int P = 32 / Q;       // position groups per warp
+    static constexpr int NW = NWARPS;      // warps per CTA
+    static constexpr int X = 8;            // positions per block
+    static constexpr int PC = NW * P * X;  // positions per CTA
+};
+
+__host__ __device__ inline int cluster2_mp(int M) { return ((M + 7) / 8) * 8; }
+
+__host__ __device__ inline size_t cluster2_smem_bytes(int M, int pc)
+{
+    const int mp = cluster2_mp(M);
+    return (size_t)((pc + 2 * mp) + 4 * mp) * 16 * 16;
+}
+
+// One step t of the tap loop for the outputs selected by ACTIVE(jj) (compile-time in the
+// prologue/epilogue).  LOAD(jj) says whether output jj starts a new tap pair at this step.
+// Packed form of IMG2D_MAC8 (sm_100 FFMA2): acc (re, im) += (fr, fr) (v.re, v.im) + (-fi, fi) (v.im, v.re).
+// va/vb hold (S.re, S.im, conj R.re, conj R.im) of slots q and q+8; sw* are the same pairs swapped.
+#define IMG2D_MAC8P(c, fr, fi, va, vb, swa0, swa1, swb0, swb1)                                      \
+    do {                                                                                            \
+        const float2 t1_ = make_float2(fr, fr), t2_ = make_float2(-(fi), fi);                       \
+        float2 *c2_ = reinterpret_cast<float2 *>(c);                                                \
+        c2_[0] = __ffma2_rn(t1_, make_float2(va.x, va.y), c2_[0]); c2_[0] = __ffma2_rn(t2_, swa0, c2_[0]); \
+        c2_[1] = __ffma2_rn(t1_, make_float2(va.z, va.w), c2_[1]); c2_[1] = __ffma2_rn(t2_, swa1, c2_[1]); \
+        c2_[2] = __ffma2_rn(t1_, make_float2(vb.x, vb.y), c2_[2]); c2_[2] = __ffma2_rn(t2_, swb0, c2_[2]); \
+        c2_[3] = __ffma2_rn(t1_, make_float2(vb.z, vb.w), c2_[3]); c2_[3] = __ffma2_rn(t2_, swb1, c2_[3]); \
+    } while (0)
+
+#define IMG2D_MAC8(c, fr, fi, va, vb)                                                   \
+    do {                                                                                \
+        c[0] = fmaf(fr, va.x, c[0]); c[0] = fmaf(-fi, va.y, c[0]);                      \
+        c[1] = fmaf(fr, va.y, c[1]); c[1] = fmaf(fi, va.x, c[1]);                       \
+        c[2] = fmaf(fr, va.z, c[2]); c[2] = fmaf(-fi, va.w, c[2]);                      \
+        c[3] = fmaf(fr, va.w, c[3]); c[3] = fmaf(fi, va.z, c[3]);                       \
+        c[4] = fmaf(fr, vb.x, c[4]); c[4] = fmaf(-fi, vb.y, c[4]);                      \
+        c[5] = fmaf(fr, vb.y, c[5]); c[5] = fmaf(fi, vb.x, c[5]);                       \
+        c[6] = fmaf(fr, vb.z, c[6]); c[6] = fmaf(-fi, vb.w, c[6]);                      \
+        c[7] = fmaf(fr, vb.w, c[7]); c[7] = fmaf(fi, vb.z, c[7]);                       \
+    } while (0)
+
+// NWARPS: warps per CTA (positions per CTA = 32 * NWARPS).  TAP_PF: operator tap pairs are loaded one
+// step ahead into a second register set.  ROW_PF: the next depth step's operator rows are prefetched
+// into L1 during the current step.
+template <int NWARPS, bool TAP_PF, bool ROW_PF, bool PACKED = false>
+__global__ void __launch_bounds__(NWARPS * 32, 1) migrate_cluster2_kernel(MigrateArgs a)
+{
+    using S = Cluster2Shape<NWARPS>;
+    constexpr int Q = S::Q, G = S::G, P = S::P, X = S::X, PC = S::PC;
+    const int M = a.M, L = 2 * a.M + 1;
+    const int MP = cluster2_mp(M);
+    const int NEXT = PC + 2 * MP;
+    extern __shared__ float4 smem[];
+    float4 *ext = smem;                     // [NEXT][G]; local position x at index x + MP
+    float4 *stg = smem + (size_t)NEXT * G;  // [parity][side][MP][G]; side 0 = left halo, 1 = right
+    __shared__ int s_item;
+
+    const unsigned crank = cluster_rank(), csize = cluster_size();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int p = lane / Q, q = lane % Q;
+    const int b = warp * P + p;  // this lane group's block: local positions [b*X, b*X+X)
+    const int c0 = (int)crank * PC;
+    const unsigned gmask = 0xffu << (p * Q);
+    float *part = a.partial ? a.partial + (long long)blockIdx.x * a.nextrap * a.nx : nullptr;
+    float *cmp = a.comp ? a.comp + (long long)blockIdx.x * a.nextrap * a.nx : nullptr;
+    const bool push_left = crank > 0 && b * X < MP;
+    const bool push_right = crank + 1 < csize && b * X + X > PC - MP;
+    const unsigned rank0_item = map_rank(&s_item, 0);
+    const float4 *tab = reinterpret_cast<const float4 *>(a.tabF);
+    const int pairs_per_row = a.tab_stride / 2;
+
+    for (;;) {
+        if (crank == 0 && threadIdx.x == 0) s_item = atomicAdd(a.counter, 1);
+        cluster_arrive();
+        cluster_wait();
+        const int it = ld_cluster_s32(rank0_item);
+        cluster_arrive();
+        cluster_wait();
+        if (it >= a.n_items) break;
+        const int2 item = a.items[it];
+        const GroupDesc grp = a.groups[item.x];
+        const int j = item.y, u0 = grp.u0, W = grp.W;
+
+        for (int i = threadIdx.x; i < (NEXT + 4 * MP) * G; i += blockDim.x) smem[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+        __syncthreads();
+        for (int k = grp.seg_begin; k < grp.seg_begin + grp.nseg; ++k) {
+            const int4 sg = a.segs[k];
+            const int r0 = sg.z - u0;
+            const int lo = max(r0, c0 - MP), hi = min(r0 + sg.w, c0 + PC + MP);
+            const cpx *ws = a.wave + a.shot_off[sg.x] + (long long)j * sg.w;
+            const cpx *rs = a.shot + a.shot_off[sg.x] + (long long)j * sg.w;
+            for (int x = lo + (int)threadIdx.x; x < hi; x += blockDim.x) {
+                const cpx Sv = ws[x - r0], Rv = rs[x - r0];
+                ext[(x - c0 + MP) * G + sg.y] = make_float4(Sv.re, Sv.im, Rv.re, -Rv.im);
+            }
+        }
+        // cluster-wide: no CTA may push step-0 halos into a peer that is still zeroing them
+        cluster_arrive();
+        cluster_wait();
+
+        const bool blk_active = c0 + b * X < W;
+        const int16_t *own_a = (blk_active && q < grp.nslots)
+                                   ? a.owner + grp.owner_off + (long long)q * grp.owner_stride + c0 + b * X
+                                   : nullptr;
+        const int16_t *own_b = (blk_active && q + Q < grp.nslots)
+                                   ? a.owner + grp.owner_off + (long long)(q + Q) * grp.owner_stride + c0 + b * X
+                                   : nullptr;
+        unsigned in_a = 0, in_b = 0;  // bit jj: output jj of slot q (q+8) is inside a shot's aperture
+        {
+            int16_t oa[X], ob[X];
+            load_owner<X>(own_a, oa);
+            load_owner<X>(own_b, ob);
+#pragma unroll
+            for (int jj = 0; jj < X; ++jj) {
+                in_a |= (oa[jj] >= 0 ? 1u : 0u) << jj;
+                in_b |= (ob[jj] >= 0 ? 1u : 0u) << jj;
+            }
+        }
+        const uint16_t *idx_j = a.idx + (long long)j * a.idx_jstride;
+        const int xg = u0 + c0 + b * X;  // model position of the block's first output
+        const bool img_lane = part && q == 0 && blk_active;
+        if (img_lane) {
+            asm volatile("prefetch.global.L1 [%0];" ::"l"(part + xg));
+            asm volatile("prefetch.global.L1 [%0];" ::"l"(cmp + xg));
+        }
+
+        for (int l = 0; l < a.nextrap; ++l) {
+            const int par = l & 1;
+            const uint16_t *idx_l = idx_j + (long long)l * a.idx_lstride;
+            int roff[X];  // first tap pair of each output's operator row
+#pragma unroll
+            for (int jj = 0; jj < X; ++jj) roff[jj] = (int)idx_l[min(xg + jj, a.nx - 1)] * pairs_per_row;
+            if (ROW_PF && l + 1 < a.nextrap) {
+                // lane q of the group fetches the 16-byte pairs of output q's next-step row into L1
+                const uint16_t *idx_n = idx_l + a.idx_lstride;
+                const float4 *rn = tab + (int)idx_n[min(xg + q, a.nx - 1)] * pairs_per_row;
+                for (int c = 0; c < pairs_per_row; c += 8) asm volatile("prefetch.global.L1 [%0];" ::"l"(rn + c));
+            }
+            if (img_lane && l + 1 < a.nextrap) {
+                asm volatile("prefetch.global.L1 [%0];" ::"l"(part + (long long)(l + 1) * a.nx + xg));
+                asm volatile("prefetch.global.L1 [%0];" ::"l"(cmp + (long long)(l + 1) * a.nx + xg));
+            }
+            float acc[X][8];
+#pragma unroll
+            for (int jj = 0; jj < X; ++jj)
+#pragma unroll
+                for (int e = 0; e < 8; ++e) acc[jj][e] = 0.f;
+            float4 tp[X];
+            const float4 *src = ext + (size_t)(b * X + MP - M) * G + q;
+
+            // prologue: t = 0 .. X-2, outputs jj <= t are active
+#pragma unroll
+            for (int t = 0; t < X - 1; ++t) {
+                const float4 va = src[(size_t)t * G];
+                const float4 vb = src[(size_t)t * G + Q];
+#pragma unroll
+                for (int jj = 0; jj < X; ++jj) {
+                    const int k = t - jj;
+                    if (k >= 0) {
+                        if ((k & 1) == 0) tp[jj] = __ldg(tab + roff[jj] + (k >> 1));
+                        const float fr = (k & 1) ? tp[jj].z : tp[jj].x;
+                        const float fi = (k & 1) ? tp[jj].w : tp[jj].y;
+                        IMG2D_MAC8(acc[jj], fr, fi, va, vb);
+                    }
+                }
+            }
+            // middle: t = X-1 .. L-1 in steps of two (odd t, then even t+1)
+            const float4 *sp = src + (size_t)(X - 1) * G;
+            const int nmid = (L - X + 1) / 2;
+            if (!TAP_PF) {
+                int kbase = X - 1;  // k of output 0 at the odd step
+                for (int u = 0; u < nmid; ++u, sp += 2 * G, kbase += 2) {
+                    {
+                        const float4 va = sp[0];
+                        const float4 vb = sp[Q];
+                        const float2 swa0 = make_float2(va.y, va.x), swa1 = make_float2(va.w, va.z);
+                        const float2 swb0 = make_float2(vb.y, vb.x), swb1 = make_float2(vb.w, vb.z);
+#pragma unroll
+                        for (int jj = 0; jj < X; ++jj) {
+                            // k = kbase - jj: even for odd jj (new pair), odd for even jj (held pair)
+                            if (jj & 1) tp[jj] = __ldg(tab + roff[jj] + ((kbase - jj) >> 1));
+                            const float fr = (jj & 1) ? tp[jj].x : tp[jj].z;
+                            const float fi = (jj & 1) ? tp[jj].y : tp[jj].w;
+                            if (PACKED) IMG2D_MAC8P(acc[jj], fr, fi, va, vb, swa0, swa1, swb0, swb1);
+                            else IMG2D_MAC8(acc[jj], fr, fi, va, vb);
+                        }
+                    }
+                    {
+                        const float4 va = sp[G];
+                        const float4 vb = sp[G + Q];
+                        const float2 swa0 = make_float2(va.y, va.x), swa1 = make_float2(va.w, va.z);
+                        const float2 swb0 = make_float2(vb.y, vb.x), swb1 = make_float2(vb.w, vb.z);
+#pragma unroll
+                        for (int jj = 0; jj < X; ++jj) {
+                            if (!(jj & 1)) tp[jj] = __ldg(tab + roff[jj] + ((kbase + 1 - jj) >> 1));
+                            const float fr = (jj & 1) ? tp[jj].z : tp[jj].x;
+                            const float fi = (jj & 1) ? tp[jj].w : tp[jj].y;
+                            if (PACKED) IMG2D_MAC8P(acc[jj], fr, fi, va, vb, swa0, swa1, swb0, swb1);
+                            else IMG2D_MAC8(acc[jj], fr, fi, va, vb);
+                        }
+                    }
+                }
+            } else {
+                // Each output's new pairs come one iteration early: iteration u uses nx_[jj] loaded
+                // during iteration u-1 (odd jj at the odd step, even jj at the even step) and loads
+                // the pair of iteration u+1 into the other register set.
+                float4 nx_[X];
+#pragma unroll
+                for (int jj = 0; jj < X; ++jj) {
+                    const int k0 = (X - 1) - jj + ((jj & 1) ? 0 : 1);  // first new pair's even k
+                    nx_[jj] = nmid > 0 ? __ldg(tab + roff[jj] + (k0 >> 1)) : make_float4(0.f, 0.f, 0.f, 0.f);
+                }
+                int kbase = X - 1;
+                for (int u = 0; u < nmid; ++u, sp += 2 * G, kbase += 2) {
+                    const bool more = u + 1 < nmid;
+                    {
+                        const float4 va = sp[0];
+                        const float4 vb = sp[Q];
+#pragma unroll
+                        for (int jj = 0; jj < X; ++jj) {
+                            if (jj & 1) {
+                                tp[jj] = nx_[jj];
+                                if (more) nx_[jj] = __ldg(tab + roff[jj] + ((kbase + 2 - jj) >> 1));
+                            }
+                            const float fr = (jj & 1) ? tp[jj].x : tp[jj].z;
+                            const float fi = (jj & 1) ? tp[jj].y : tp[jj].w;
+                            IMG2D_MAC8(acc[jj], fr, fi, va, vb);
+                        }
+                    }
+                    {
+                        const float4 va = sp[G];
+                        const float4 vb = sp[G + Q];
+#pragma unroll
+                        for (int jj = 0; jj < X; ++jj) {
+                            if (!(jj & 1)) {
+                                tp[jj] = nx_[jj];
+                                if (more) nx_[jj] = __ldg(tab + roff[jj] + ((kbase + 3 - jj) >> 1));
+                            }
+                            const float fr = (jj & 1) ? tp[jj].z : tp[jj].x;
+                            const float fi = (jj & 1) ? tp[jj].w : tp[jj].y;
+                            IMG2D_MAC8(acc[jj], fr, fi, va, vb);
+                        }
+                    }
+                }
+            }
+            // epilogue: t = L .. L+X-2, outputs jj > t-L are active (k = t - jj <= L-1)
+            const float4 *ep = src + (size_t)L * G;
+#pragma unroll
+            for (int e = 0; e < X - 1; ++e) {
+                const float4 va = ep[(size_t)e * G];
+                const float4 vb = ep[(size_t)e * G + Q];
+#pragma unroll
+                for (int jj = 0; jj < X; ++jj) {
+                    if (jj > e) {
+                        // k = L + e - jj, parity of (1 + e - jj) since L is odd
+                        const bool even = ((1 + e - jj) & 1) == 0;
+                        if (even) tp[jj] = __ldg(tab + roff[jj] + ((L + e - jj) >> 1));
+                        const float fr = even ? tp[jj].x : tp[jj].z;
+                        const float fi = even ? tp[jj].y : tp[jj].w;
+                        IMG2D_MAC8(acc[jj], fr, fi, va, vb);
+                    }
+                }
+            }
+#pragma unroll
+            for (int jj = 0; jj < X; ++jj) {
+                if (!((in_a >> jj) & 1u)) acc[jj][0] = acc[jj][1] = acc[jj][2] = acc[jj][3] = 0.f;
+                if (!((in_b >> jj) & 1u)) acc[jj][4] = acc[jj][5] = acc[jj][6] = acc[jj][7] = 0.f;
+            }
+            // halos of step l+1 into the neighbours' staging (parity par^1); see wlsq_cluster.cuh
+            if (push_left) {
+                float4 *dst = stg + ((size_t)((par ^ 1) * 2 + 1) * MP) * G;
+#pragma unroll
+                for (int jj = 0; jj < X; ++jj) {
+                    const int x = b * X + jj;
+                    if (x < MP) {
+                        const unsigned ra = map_rank(dst + (size_t)x * G + q, crank - 1);
+                        st_cluster(ra, make_float4(acc[jj][0], acc[jj][1], acc[jj][2], acc[jj][3]));
+                        st_cluster(ra + Q * 16, make_float4(acc[jj][4], acc[jj][5], acc[jj][6], acc[jj][7]));
+                    }
+                }
+            }
+            if (push_right) {
+                float4 *dst = stg + ((size_t)((par ^ 1) * 2 + 0) * MP) * G;
+#pragma unroll
+                for (int jj = 0; jj < X; ++jj) {
+                    const int x = b * X + jj - (PC - MP);
+                    if (x >= 0) {
+                        const unsigned ra = map_rank(dst + (size_t)x * G + q, crank + 1);
+                        st_cluster(ra, make_float4(acc[jj][0], acc[jj][1], acc[jj][2], acc[jj][3]));
+                        st_cluster(ra + Q * 16, make_float4(acc[jj][4], acc[jj][5], acc[jj][6], acc[jj][7]));
+                    }
+                }
+            }
+            __syncthreads();  // every read of step l's values in ext[] is done
+            float4 *dst = ext + (size_t)(b * X + MP) * G + q;
+#pragma unroll
+            for (int jj = 0; jj < X; ++jj) {
+                dst[(size_t)jj * G] = make_float4(acc[jj][0], acc[jj][1], acc[jj][2], acc[jj][3]);
+                dst[(size_t)jj * G + Q] = make_float4(acc[jj][4], acc[jj][5], acc[jj][6], acc[jj][7]);
+            }
+            cluster_arrive();
+            float *prow = part ? part + (long long)l * a.nx : nullptr;
+            float *crow = cmp ? cmp + (long long)l * a.nx : nullptr;
+#pragma unroll
+            for (int jj = 0; jj < X; ++jj) {
+                const float ia = acc[jj][0] * acc[jj][2] - acc[jj][1] * acc[jj][3];
+                const float ib = acc[jj][4] * acc[jj][6] - acc[jj][5] * acc[jj][7];
+                if (a.image_shots) {
+                    // per-shot images (optional output): shot ids re-read from the owner table
+                    if ((in_a >> jj) & 1u)
+                        atomicAdd(a.image_shots + (long long)own_a[jj] * a.img_sstride + (long long)l * a.nx + xg + jj, ia);
+                    if ((in_b >> jj) & 1u)
+                        atomicAdd(a.image_shots + (long long)own_b[jj] * a.img_sstride + (long long)l * a.nx + xg + jj, ib);
+                }
+                float img = ia + ib;
+#pragma unroll
+                for (int off = 1; off < Q; off <<= 1) img += __shfl_xor_sync(gmask, img, off);
+                if (prow && q == 0 && c0 + b * X + jj < W) kahan_add(prow + xg + jj, crow + xg + jj, img);
+            }
+            cluster_wait();
+            const float4 *hs = stg + (size_t)((par ^ 1) * 2) * MP * G;
+            for (int i = threadIdx.x; i < 2 * MP * G; i += blockDim.x) {
+                const int side = i / (MP * G), r = i % (MP * G);
+                ext[(side ? (PC + MP) * G : 0) + r] = hs[i];
+            }
+            __syncthreads();
+        }
+        if (a.write_back) {
+            for (int k = grp.seg_begin; k < grp.seg_begin + grp.nseg; ++k) {
+                const int4 sg = a.segs[k];
+                const int r0 = sg.z - u0;
+                const int lo = max(r0, c0), hi = min(r0 + sg.w, c0 + PC);
+                cpx *ws = a.wave + a.shot_off[sg.x] + (long long)j * sg.w;
+                cpx *rs = a.shot + a.shot_off[sg.x] + (long long)j * sg.w;
+                for (int x = lo + (int)threadIdx.x; x < hi; x += blockDim.x) {
+                    const float4 v = ext[(x - c0 + MP) * G + sg.y];
+                    ws[x - r0] = cpx{v.x, v.y};
+                    rs[x - r0] = cpx{v.z, -v.w};
+                }
+            }
+        }
+        __syncthreads();
+    }
+    cluster_arrive();
+    cluster_wait();
+}
+
+#undef IMG2D_MAC8
+#undef IMG2D_MAC8P
+
+}  // namespace img2d

@@ -15,7 +15,7 @@ from ._lib import check, lib, ptr
 
 def migrate(ns, nextrap, nz, nx, nf, nt, M, nk, dk, omega, velocity, tab_forw, wave_fs, shot_fs,
             tab_back=None, shot_x0=None, shot_nx=None, image=True, image_shots=False, two_tables=False,
-            generic=False, no_cluster=False):
+            generic=False, no_cluster=False, cluster_v1=False):
     """Host-buffer migration.  wave_fs/shot_fs (packed complex64) are overwritten with the final
     wavefields.  Returns (image (nz, nx) float32 or None, image_shots (ns, nz, nx) or None); rows
     [nextrap, nz) are zero."""
@@ -32,20 +32,22 @@ def migrate(ns, nextrap, nz, nx, nf, nt, M, nk, dk, omega, velocity, tab_forw, w
     img = np.zeros((nz, nx), dtype=np.float32) if image else None
     imgs = np.zeros((ns, nz, nx), dtype=np.float32) if image_shots else None
     flags = (_lib.FLAG_TWO_TABLES if two_tables else 0) | (_lib.FLAG_GENERIC if generic else 0) | \
-        (_lib.FLAG_NO_CLUSTER if no_cluster else 0)
+        (_lib.FLAG_NO_CLUSTER if no_cluster else 0) | (_lib.FLAG_CLUSTER_V1 if cluster_v1 else 0)
     check(lib().img2d_migrate_compact(ns, nextrap, nz, nx, nf, nt, M, nk, float(dk), ptr(omega), ptr(velocity),
                                       ptr(tab_forw), ptr(tab_back), ptr(x0), ptr(wn), ptr(wave_fs), ptr(shot_fs),
                                       ptr(img), ptr(imgs), flags))
     return img, imgs
 
 
-def migrate_workload(w, two_tables=False, table_back=None, image_shots=False, generic=False, no_cluster=False):
+def migrate_workload(w, two_tables=False, table_back=None, image_shots=False, generic=False, no_cluster=False,
+                     cluster_v1=False):
     """Run a synthetic.Workload through the host entry point on copies of its spectra."""
     wave = w.wave.copy()
     shot = w.shot.copy()
     img, imgs = migrate(w.ns, w.nextrap, w.nz, w.nx, w.nf, w.nt, w.M, w.nk, w.dk, w.omega, w.velocity, w.table,
                         wave, shot, tab_back=table_back, shot_x0=w.shot_x0, shot_nx=w.shot_nx,
-                        image_shots=image_shots, two_tables=two_tables, generic=generic, no_cluster=no_cluster)
+                        image_shots=image_shots, two_tables=two_tables, generic=generic, no_cluster=no_cluster,
+                        cluster_v1=cluster_v1)
     return img, imgs, wave, shot
 
 
@@ -60,13 +62,14 @@ class Plan:
     """Device-resident migration plan (torch CUDA tensors in, torch CUDA tensors out)."""
 
     def __init__(self, ns, nextrap, nz, nx, nf, nt, M, nk, shot_x0=None, shot_nx=None, two_tables=False,
-                 generic=False, no_cluster=False):
+                 generic=False, no_cluster=False, cluster_v1=False, variant=0):
         self.ns, self.nextrap, self.nz, self.nx, self.nf, self.nt, self.M, self.nk = \
             ns, nextrap, nz, nx, nf, nt, M, nk
         x0 = None if shot_x0 is None else np.ascontiguousarray(shot_x0, dtype=np.int32)
         wn = None if shot_nx is None else np.ascontiguousarray(shot_nx, dtype=np.int32)
         flags = (_lib.FLAG_TWO_TABLES if two_tables else 0) | (_lib.FLAG_GENERIC if generic else 0) | \
-            (_lib.FLAG_NO_CLUSTER if no_cluster else 0)
+            (_lib.FLAG_NO_CLUSTER if no_cluster else 0) | (_lib.FLAG_CLUSTER_V1 if cluster_v1 else 0) | \
+            (int(variant) << _lib.FLAG_VARIANT_SHIFT)
         h = ctypes.c_void_p()
         check(lib().img2d_plan_create(ctypes.byref(h), ns, nextrap, nz, nx, nf, nt, M, nk, ptr(x0), ptr(wn), flags))
         self._h = h

@@ -37,6 +37,10 @@ typedef struct {
 #define IMG2D_FLAG_TWO_TABLES 1   /* use tab_back for the receiver instead of conj(tab_forw) */
 #define IMG2D_FLAG_GENERIC 2      /* force the runtime-length kernel (testing) */
 #define IMG2D_FLAG_NO_CLUSTER 4   /* use the single-CTA kernels even where the cluster kernel applies */
+#define IMG2D_FLAG_CLUSTER_V1 8   /* first-generation cluster kernel (256 threads, fixed L) instead */
+/* select variant v (1-based; 0 = default) of the second-generation cluster kernel: bits 8-15 */
+#define IMG2D_FLAG_VARIANT_SHIFT 8
+#define IMG2D_FLAG_VARIANT(v) ((v) << IMG2D_FLAG_VARIANT_SHIFT)
 
 const char *img2d_last_error(void);
 int img2d_version(void);

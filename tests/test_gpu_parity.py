@@ -213,25 +213,51 @@ def test_invalid_arguments_raise():
         migration.Plan(w.ns, w.nz + 1, w.nz, w.nx, w.nf, w.nt, w.M, w.nk)
 
 
+@pytest.mark.parametrize("v1", [False, True], ids=["cluster2", "cluster1"])
 @pytest.mark.parametrize("kind,nx,nz,nf,ns", [("medium", 256, 12, 6, 16), ("medium", 480, 10, 5, 24),
                                               ("uneven", 1000, 8, 5, 40), ("uneven", 2048, 6, 4, 64),
-                                              ("medium", 2048, 5, 3, 32)])
-def test_cluster_kernel_matches_oracle_and_single_cta(kind, nx, nz, nf, ns):
-    """Clusters of 1, 2, 4 and 8 CTAs (256 positions each) against the FP64 oracle and against the
-    single-CTA kernel; few depth steps and frequencies keep the oracle fast."""
+                                              ("medium", 2048, 5, 3, 32), ("medium", 3000, 4, 3, 20)])
+def test_cluster_kernel_matches_oracle_and_single_cta(kind, nx, nz, nf, ns, v1):
+    """Both cluster kernels (256 positions per CTA for the first, 512 for the second; clusters of
+    1 to 8 CTAs) against the FP64 oracle and against the single-CTA kernel; few depth steps and
+    frequencies keep the oracle fast."""
     if kind == "medium":
         w = synthetic.plain_medium(nx=nx, nz=nz, nf=nf, ns=ns, scale=1.0)
     else:
         w = synthetic.batched_uneven(nx=nx, nz=nz, nf=nf, ns=ns, scale=1.0)
-    plan = migration.Plan.for_workload(w)
+    plan = migration.Plan.for_workload(w, cluster_v1=v1)
     d = plan.describe()
     plan.close()
-    assert d["kernel"] == "migrate_cluster", d
-    assert d["cluster"] == {256: 1, 480: 2, 1000: 4, 2048: 8}[nx] or kind == "uneven", d
-    img, imgs, wave, shot = migration.migrate_workload(w, image_shots=True)
+    if v1 and nx > 2048:
+        assert d["kernel"] != "migrate_cluster", d  # 8 CTAs x 256 positions do not cover it
+        return
+    assert d["kernel"] == ("migrate_cluster" if v1 else "migrate_cluster2"), d
+    pc = 256 if v1 else 512
+    if kind == "medium":
+        assert d["cluster"] >= -(-nx // pc), d
+    img, imgs, wave, shot = migration.migrate_workload(w, image_shots=True, cluster_v1=v1)
     e = _compact_check(w, img, wave, shot)
     img1, _, wave1, _ = migration.migrate_workload(w, no_cluster=True)
     assert rel_l2(img, img1) <= 2e-6 and rel_l2(wave, wave1) <= 2e-6
     _, shots_o, _, _ = oracle.migrate_workload_f64(w)
     assert rel_l2(imgs, shots_o) <= 1e-5
     assert e <= 1e-5
+
+
+@pytest.mark.parametrize("variant", [1, 2, 3, 4, 5, 6, 7])
+def test_cluster2_variants_match_oracle(variant):
+    """Every variant of the second-generation cluster kernel (warps per CTA, operator-pair
+    prefetch, L1 row prefetch) on a window that needs a multi-CTA cluster."""
+    w = synthetic.batched_uneven(nx=1500, nz=7, nf=4, ns=48, scale=1.0)
+    plan = migration.Plan.for_workload(w, variant=variant)
+    d = plan.describe()
+    plan.close()
+    assert d["kernel"] == "migrate_cluster2" and d["variant"] == variant - 1 and d["cluster"] >= 2, d
+    wave, shot = w.wave.copy(), w.shot.copy()
+    from imaging2d_wlsq_b200._lib import FLAG_VARIANT_SHIFT, check, lib, ptr
+    img = np.zeros((w.nz, w.nx), dtype=np.float32)
+    check(lib().img2d_migrate_compact(w.ns, w.nextrap, w.nz, w.nx, w.nf, w.nt, w.M, w.nk, float(w.dk), ptr(w.omega),
+                                      ptr(np.ascontiguousarray(w.velocity)), ptr(w.table), None,
+                                      ptr(np.ascontiguousarray(w.shot_x0)), ptr(np.ascontiguousarray(w.shot_nx)),
+                                      ptr(wave), ptr(shot), ptr(img), None, variant << FLAG_VARIANT_SHIFT))
+    _compact_check(w, img, wave, shot)
