@@ -25,6 +25,8 @@ FLAG_GENERIC = 2
 FLAG_NO_CLUSTER = 4
 FLAG_CLUSTER_V1 = 8
 FLAG_VARIANT_SHIFT = 8
+FLAG_TABLE_FP16 = 16
+FLAG_TABLE_BF16 = 32
 NOALLOC_SCRATCH_BYTES = 64 << 20
 
 ERROR_NAMES = {1: "EINVAL", 2: "ENOMEM", 3: "ECUDA", 4: "ENODEV"}

@@ -259,11 +259,12 @@ struct img2d_plan {
     int cluster = 0;  // CTAs per cluster of the cluster kernel, 0 = single-CTA kernels
     int block = 256;                  // threads per CTA of the chosen kernel
     int variant = -1;                 // index into the cluster2 variant table
+    int tab16 = 0;                    // operator table storage: 0 FP32, 1 FP16, 2 BF16
     const char *kname = "";           // name of the chosen kernel
     img2d::Carver *carver = nullptr;  // no-allocation mode: buffers carved from fixed scratch
     cudaStream_t upload_stream = 0;   // no-allocation mode: stream of the descriptor uploads
     bool timing = true;               // record events around the migration kernel
-    img2d::DevBuf items, groups, segs, owner, shot_off, idx, tabF, tabB, partial, comp, counter, naive_buf;
+    img2d::DevBuf items, groups, segs, owner, shot_off, idx, tabF, tabB, tab16buf, partial, comp, counter, naive_buf;
     // dense tables (drop-in ABI) are owned by the caller of run_dense
 };
 
@@ -405,7 +406,15 @@ static int build_plan(img2d_plan *p, int ns, int nextrap, int nz, int nx, int nf
                             p->n_slots >= 12;
     int vsel = (flags >> IMG2D_FLAG_VARIANT_SHIFT) & 0xff;
     vsel = (vsel >= 1 && vsel <= kNumCluster2) ? vsel - 1 : kCluster2Default;
-    const Cluster2Variant &cv = kCluster2[vsel];
+    Cluster2Variant cv = kCluster2[vsel];
+    const int tab16 = (flags & IMG2D_FLAG_TABLE_BF16) ? 2 : ((flags & IMG2D_FLAG_TABLE_FP16) ? 1 : 0);
+    if (tab16) {
+        // reduced-precision operator storage: default shape with 16-bit tap loads
+        cv = {16, false, false,
+              tab16 == 1 ? migrate_cluster2_kernel<16, false, false, false, TAB_F16>
+                         : migrate_cluster2_kernel<16, false, false, false, TAB_BF16>};
+        vsel = kCluster2Default;
+    }
     const int pc2 = cv.nw * 32;
     if (cluster_ok && !(flags & IMG2D_FLAG_CLUSTER_V1) && p->L >= 7 &&
         cluster2_smem_bytes(M, pc2) + static_reserve <= (size_t)smem_optin) {
@@ -423,6 +432,10 @@ static int build_plan(img2d_plan *p, int ns, int nextrap, int nz, int nx, int nf
             p->kname = "migrate_cluster2";
         }
     }
+    if (tab16 && !p->cluster)
+        return fail(IMG2D_EINVAL, "16-bit operator tables need the cluster kernel (>= 12 lane slots, 2M+1 >= 7, "
+                                  "window <= 8 CTAs)");
+    p->tab16 = tab16;
     const ClusterKernel *ck = cluster_ok ? find_cluster(p->L) : nullptr;
     if (!p->cluster && ck && ck->smem + static_reserve <= (size_t)smem_optin) {
         const int widest = make_groups(ClusterShape::G);
@@ -527,6 +540,7 @@ static int build_plan(img2d_plan *p, int ns, int nextrap, int nz, int nx, int nf
         if ((rc = p->idx.ensure((size_t)nf * nextrap * p->idx_lstride * sizeof(uint16_t)))) return rc;
         p->tab_stride = (p->L + 1) / 2 * 2;
         if ((rc = p->tabF.ensure((size_t)nk * p->tab_stride * sizeof(cpx)))) return rc;
+        if (p->tab16 && (rc = p->tab16buf.ensure((size_t)nk * p->tab_stride * sizeof(unsigned)))) return rc;
         if (mode == OP_TWO && (rc = p->tabB.ensure((size_t)nk * p->tab_stride * sizeof(cpx)))) return rc;
     }
     return IMG2D_OK;
@@ -548,6 +562,7 @@ static MigrateArgs base_args(img2d_plan *p, cpx *wave, cpx *shot)
     a.shot_off = p->shot_off.as<long long>();
     a.tabF = p->tabF.as<cpx>();
     a.tabB = p->mode == OP_TWO ? p->tabB.as<cpx>() : p->tabF.as<cpx>();
+    a.tab16 = p->tab16buf.p;
     a.idx = p->idx.as<uint16_t>();
     a.idx_jstride = (long long)p->nextrap * p->idx_lstride;
     a.idx_lstride = p->idx_lstride;
@@ -624,6 +639,12 @@ static int set_model(img2d_plan *p, const double *d_omega, const double *d_vel, 
     if (p->mode == OP_TWO) {
         IMG2D_CUDA(cudaMemsetAsync(p->tabB.p, 0, (size_t)p->nk * prow, st));
         IMG2D_CUDA(cudaMemcpy2DAsync(p->tabB.p, prow, d_tabB, row, row, p->nk, cudaMemcpyDeviceToDevice, st));
+    }
+    if (p->tab16) {
+        const long long n = (long long)p->nk * p->tab_stride;
+        table_to_16bit_kernel<<<(int)std::min<long long>((n + 255) / 256, 148 * 8), 256, 0, st>>>(
+            p->tabF.as<cpx>(), n, p->tab16 == 2, p->tab16buf.as<unsigned>());
+        IMG2D_CUDA(cudaGetLastError());
     }
     const long long total = (long long)p->nf * p->nextrap * p->nx;
     const int blocks = (int)std::min<long long>((total + 255) / 256, 148 * 16);
@@ -805,7 +826,7 @@ size_t img2d_plan_workspace_bytes(const img2d_plan *p)
 {
     if (!p) return 0;
     return p->items.bytes + p->groups.bytes + p->segs.bytes + p->owner.bytes + p->shot_off.bytes +
-           p->idx.bytes + p->tabF.bytes + p->tabB.bytes + p->partial.bytes + p->comp.bytes + p->counter.bytes +
+           p->idx.bytes + p->tabF.bytes + p->tabB.bytes + p->tab16buf.bytes + p->partial.bytes + p->comp.bytes + p->counter.bytes +
            p->naive_buf.bytes;
 }
 
@@ -814,9 +835,11 @@ int img2d_plan_describe(const img2d_plan *p, char *buf, int buflen)
     if (!p || !buf || buflen <= 0) return fail(IMG2D_EINVAL, "bad describe arguments");
     snprintf(buf, buflen,
              "{\"kernel\": \"%s\", \"cluster\": %d, \"G\": %d, \"X\": %d, \"L\": %d, \"grid\": %d, \"block\": %d, "
-             "\"smem\": %zu, \"items\": %d, \"slots\": %d, \"max_union_width\": %d, \"mode\": %d, \"variant\": %d}",
+             "\"smem\": %zu, \"items\": %d, \"slots\": %d, \"max_union_width\": %d, \"mode\": %d, \"variant\": %d, "
+             "\"table\": \"%s\"}",
              p->kname, p->cluster, p->G, p->fixed ? kX : 4, p->L, p->grid, p->block, p->smem,
-             p->n_items, p->n_slots, p->max_w, p->mode, p->variant);
+             p->n_items, p->n_slots, p->max_w, p->mode, p->variant,
+             p->tab16 == 2 ? "bf16" : (p->tab16 == 1 ? "fp16" : "fp32"));
     return IMG2D_OK;
 }
 
@@ -924,7 +947,7 @@ int img2d_migrate_compact_noalloc(int ns, int nextrap, int nz, int nx, int nf, i
     plan.upload_stream = (cudaStream_t)stream;
     plan.timing = false;
     for (DevBuf *b : {&plan.items, &plan.groups, &plan.segs, &plan.owner, &plan.shot_off, &plan.idx, &plan.tabF,
-                      &plan.tabB, &plan.partial, &plan.comp, &plan.counter, &plan.naive_buf})
+                      &plan.tabB, &plan.tab16buf, &plan.partial, &plan.comp, &plan.counter, &plan.naive_buf})
         b->carver = &carver;
     if ((rc = build_plan(&plan, ns, nextrap, nz, nx, nf, nt, M, nk, shot_x0, shot_nx, IMG2D_FLAG_NO_CLUSTER, OP_CONJ)))
         return rc;

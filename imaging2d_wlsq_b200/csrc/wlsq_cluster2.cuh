@@ -64,10 +64,31 @@ __host__ __device__ inline size_t cluster2_smem_bytes(int M, int pc)
         c[7] = fmaf(fr, vb.w, c[7]); c[7] = fmaf(fi, vb.z, c[7]);                       \
     } while (0)
 
+// Operator-table storage of the cluster kernel: complex64 taps, or (re, im) pairs in FP16 / BF16
+// (4 bytes per tap, widened to FP32 in registers; the arithmetic stays FP32).
+enum TableType : int { TAB_F32 = 0, TAB_F16 = 1, TAB_BF16 = 2 };
+
+// Taps (2i, 2i+1) of a row as one float4 (re0, im0, re1, im1).
+template <int TT>
+__device__ __forceinline__ float4 load_tap_pair(const void *row, int i)
+{
+    if (TT == TAB_F32) return __ldg(reinterpret_cast<const float4 *>(row) + i);
+    const uint2 u = __ldg(reinterpret_cast<const uint2 *>(row) + i);
+    float2 a, b;
+    if (TT == TAB_F16) {
+        a = __half22float2(*reinterpret_cast<const __half2 *>(&u.x));
+        b = __half22float2(*reinterpret_cast<const __half2 *>(&u.y));
+    } else {
+        a = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162 *>(&u.x));
+        b = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162 *>(&u.y));
+    }
+    return make_float4(a.x, a.y, b.x, b.y);
+}
+
 // NWARPS: warps per CTA (positions per CTA = 32 * NWARPS).  TAP_PF: operator tap pairs are loaded one
 // step ahead into a second register set.  ROW_PF: the next depth step's operator rows are prefetched
 // into L1 during the current step.
-template <int NWARPS, bool TAP_PF, bool ROW_PF, bool PACKED = false>
+template <int NWARPS, bool TAP_PF, bool ROW_PF, bool PACKED = false, int TT = TAB_F32>
 __global__ void __launch_bounds__(NWARPS * 32, 1) migrate_cluster2_kernel(MigrateArgs a)
 {
     using S = Cluster2Shape<NWARPS>;
@@ -91,8 +112,9 @@ __global__ void __launch_bounds__(NWARPS * 32, 1) migrate_cluster2_kernel(Migrat
     const bool push_left = crank > 0 && b * X < MP;
     const bool push_right = crank + 1 < csize && b * X + X > PC - MP;
     const unsigned rank0_item = map_rank(&s_item, 0);
-    const float4 *tab = reinterpret_cast<const float4 *>(a.tabF);
-    const int pairs_per_row = a.tab_stride / 2;
+    // row r starts at byte r * row_bytes; taps are addressed in pairs through load_tap_pair
+    const char *tabb = reinterpret_cast<const char *>(TT == TAB_F32 ? (const void *)a.tabF : a.tab16);
+    const int row_bytes = a.tab_stride * (TT == TAB_F32 ? 8 : 4);
 
     for (;;) {
         if (crank == 0 && threadIdx.x == 0) s_item = atomicAdd(a.counter, 1);
@@ -152,14 +174,14 @@ __global__ void __launch_bounds__(NWARPS * 32, 1) migrate_cluster2_kernel(Migrat
         for (int l = 0; l < a.nextrap; ++l) {
             const int par = l & 1;
             const uint16_t *idx_l = idx_j + (long long)l * a.idx_lstride;
-            int roff[X];  // first tap pair of each output's operator row
+            int roff[X];  // byte offset of each output's operator row
 #pragma unroll
-            for (int jj = 0; jj < X; ++jj) roff[jj] = (int)idx_l[min(xg + jj, a.nx - 1)] * pairs_per_row;
+            for (int jj = 0; jj < X; ++jj) roff[jj] = (int)idx_l[min(xg + jj, a.nx - 1)] * row_bytes;
             if (ROW_PF && l + 1 < a.nextrap) {
                 // lane q of the group fetches the 16-byte pairs of output q's next-step row into L1
                 const uint16_t *idx_n = idx_l + a.idx_lstride;
-                const float4 *rn = tab + (int)idx_n[min(xg + q, a.nx - 1)] * pairs_per_row;
-                for (int c = 0; c < pairs_per_row; c += 8) asm volatile("prefetch.global.L1 [%0];" ::"l"(rn + c));
+                const char *rn = tabb + (long long)idx_n[min(xg + q, a.nx - 1)] * row_bytes;
+                for (int c = 0; c < row_bytes; c += 128) asm volatile("prefetch.global.L1 [%0];" ::"l"(rn + c));
             }
             if (img_lane && l + 1 < a.nextrap) {
                 asm volatile("prefetch.global.L1 [%0];" ::"l"(part + (long long)(l + 1) * a.nx + xg));
@@ -182,7 +204,7 @@ __global__ void __launch_bounds__(NWARPS * 32, 1) migrate_cluster2_kernel(Migrat
                 for (int jj = 0; jj < X; ++jj) {
                     const int k = t - jj;
                     if (k >= 0) {
-                        if ((k & 1) == 0) tp[jj] = __ldg(tab + roff[jj] + (k >> 1));
+                        if ((k & 1) == 0) tp[jj] = load_tap_pair<TT>(tabb + roff[jj], (k >> 1));
                         const float fr = (k & 1) ? tp[jj].z : tp[jj].x;
                         const float fi = (k & 1) ? tp[jj].w : tp[jj].y;
                         IMG2D_MAC8(acc[jj], fr, fi, va, vb);
@@ -203,7 +225,7 @@ __global__ void __launch_bounds__(NWARPS * 32, 1) migrate_cluster2_kernel(Migrat
 #pragma unroll
                         for (int jj = 0; jj < X; ++jj) {
                             // k = kbase - jj: even for odd jj (new pair), odd for even jj (held pair)
-                            if (jj & 1) tp[jj] = __ldg(tab + roff[jj] + ((kbase - jj) >> 1));
+                            if (jj & 1) tp[jj] = load_tap_pair<TT>(tabb + roff[jj], ((kbase - jj) >> 1));
                             const float fr = (jj & 1) ? tp[jj].x : tp[jj].z;
                             const float fi = (jj & 1) ? tp[jj].y : tp[jj].w;
                             if (PACKED) IMG2D_MAC8P(acc[jj], fr, fi, va, vb, swa0, swa1, swb0, swb1);
@@ -217,7 +239,7 @@ __global__ void __launch_bounds__(NWARPS * 32, 1) migrate_cluster2_kernel(Migrat
                         const float2 swb0 = make_float2(vb.y, vb.x), swb1 = make_float2(vb.w, vb.z);
 #pragma unroll
                         for (int jj = 0; jj < X; ++jj) {
-                            if (!(jj & 1)) tp[jj] = __ldg(tab + roff[jj] + ((kbase + 1 - jj) >> 1));
+                            if (!(jj & 1)) tp[jj] = load_tap_pair<TT>(tabb + roff[jj], ((kbase + 1 - jj) >> 1));
                             const float fr = (jj & 1) ? tp[jj].z : tp[jj].x;
                             const float fi = (jj & 1) ? tp[jj].w : tp[jj].y;
                             if (PACKED) IMG2D_MAC8P(acc[jj], fr, fi, va, vb, swa0, swa1, swb0, swb1);
@@ -233,7 +255,7 @@ __global__ void __launch_bounds__(NWARPS * 32, 1) migrate_cluster2_kernel(Migrat
 #pragma unroll
                 for (int jj = 0; jj < X; ++jj) {
                     const int k0 = (X - 1) - jj + ((jj & 1) ? 0 : 1);  // first new pair's even k
-                    nx_[jj] = nmid > 0 ? __ldg(tab + roff[jj] + (k0 >> 1)) : make_float4(0.f, 0.f, 0.f, 0.f);
+                    nx_[jj] = nmid > 0 ? load_tap_pair<TT>(tabb + roff[jj], (k0 >> 1)) : make_float4(0.f, 0.f, 0.f, 0.f);
                 }
                 int kbase = X - 1;
                 for (int u = 0; u < nmid; ++u, sp += 2 * G, kbase += 2) {
@@ -245,7 +267,7 @@ __global__ void __launch_bounds__(NWARPS * 32, 1) migrate_cluster2_kernel(Migrat
                         for (int jj = 0; jj < X; ++jj) {
                             if (jj & 1) {
                                 tp[jj] = nx_[jj];
-                                if (more) nx_[jj] = __ldg(tab + roff[jj] + ((kbase + 2 - jj) >> 1));
+                                if (more) nx_[jj] = load_tap_pair<TT>(tabb + roff[jj], ((kbase + 2 - jj) >> 1));
                             }
                             const float fr = (jj & 1) ? tp[jj].x : tp[jj].z;
                             const float fi = (jj & 1) ? tp[jj].y : tp[jj].w;
@@ -259,7 +281,7 @@ __global__ void __launch_bounds__(NWARPS * 32, 1) migrate_cluster2_kernel(Migrat
                         for (int jj = 0; jj < X; ++jj) {
                             if (!(jj & 1)) {
                                 tp[jj] = nx_[jj];
-                                if (more) nx_[jj] = __ldg(tab + roff[jj] + ((kbase + 3 - jj) >> 1));
+                                if (more) nx_[jj] = load_tap_pair<TT>(tabb + roff[jj], ((kbase + 3 - jj) >> 1));
                             }
                             const float fr = (jj & 1) ? tp[jj].z : tp[jj].x;
                             const float fi = (jj & 1) ? tp[jj].w : tp[jj].y;
@@ -279,7 +301,7 @@ __global__ void __launch_bounds__(NWARPS * 32, 1) migrate_cluster2_kernel(Migrat
                     if (jj > e) {
                         // k = L + e - jj, parity of (1 + e - jj) since L is odd
                         const bool even = ((1 + e - jj) & 1) == 0;
-                        if (even) tp[jj] = __ldg(tab + roff[jj] + ((L + e - jj) >> 1));
+                        if (even) tp[jj] = load_tap_pair<TT>(tabb + roff[jj], ((L + e - jj) >> 1));
                         const float fr = even ? tp[jj].x : tp[jj].z;
                         const float fi = even ? tp[jj].y : tp[jj].w;
                         IMG2D_MAC8(acc[jj], fr, fi, va, vb);

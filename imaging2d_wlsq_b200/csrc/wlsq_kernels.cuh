@@ -24,6 +24,8 @@
 // compensation (no global atomics on the stacked image).  A persistent grid pulls work items
 // from an atomic counter; a final kernel sums the per-CTA partials.
 #pragma once
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -64,6 +66,7 @@ struct MigrateArgs {
     const long long *shot_off;  // element offset of each shot's block in wave/shot
     const cpx *tabF;
     const cpx *tabB;
+    const void *tab16;       // 16-bit copy of tabF (FP16 or BF16 (re, im) pairs), same row stride
     const uint16_t *idx;     // [nf][nextrap][idx_lstride] compact row index
     long long idx_jstride;
     int idx_lstride;
@@ -428,6 +431,22 @@ __global__ void reduce_partials_kernel(const float *__restrict__ partial, const 
             kahan_add(&s, &c, v);
         }
         image[e] = s - c;
+    }
+}
+
+// 16-bit copy of the padded operator table: (re, im) of each tap as half2 / bfloat162, rounded to
+// nearest.  Used by the reduced-precision table storage modes of the cluster kernel.
+__global__ void table_to_16bit_kernel(const cpx *__restrict__ src, long long n, int bf16, unsigned *__restrict__ dst)
+{
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+        const cpx v = src[e];
+        if (bf16) {
+            const __nv_bfloat162 h = __floats2bfloat162_rn(v.re, v.im);
+            dst[e] = *reinterpret_cast<const unsigned *>(&h);
+        } else {
+            const __half2 h = __floats2half2_rn(v.re, v.im);
+            dst[e] = *reinterpret_cast<const unsigned *>(&h);
+        }
     }
 }
 

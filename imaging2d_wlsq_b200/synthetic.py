@@ -174,8 +174,8 @@ def batched_uneven(seed=3, scale=1.0, tables=True, ns=256, nz=None, nx=None, nf=
     return _finish(w, 2.0, 50.0, 20.0, rng, tables)
 
 
-def precision(seed=4, scale=1.0, tables=True, ns=64, nextrap=None):
-    nz, nx = max(8, int(2000 * scale)), max(64, int(4096 * scale))
+def precision(seed=4, scale=1.0, tables=True, ns=64, nextrap=None, nf=None, nx=None):
+    nz, nx = max(8, int(2000 * scale)), nx or max(64, int(4096 * scale))
     rng = np.random.default_rng(seed)
     v = gaussian_random_field(nz, nx, 50.0 * max(scale, 0.1), 1500.0, 4500.0, rng)
     for _ in range(20):
@@ -186,7 +186,7 @@ def precision(seed=4, scale=1.0, tables=True, ns=64, nextrap=None):
     ns = max(2, int(ns * scale)) if scale < 1.0 else ns
     pos = np.linspace(nx / (2 * ns), nx - nx / (2 * ns), ns).astype(np.int32)
     x0, wdt, pos = _full_aperture(ns, nx, pos)
-    w = Workload("precision", nz, nx, 5.0, 5.0, max(4, int(1024 * scale)), 27, max(64, int(8000 * scale)), 0.0,
+    w = Workload("precision", nz, nx, 5.0, 5.0, nf or max(4, int(1024 * scale)), 27, max(64, int(8000 * scale)), 0.0,
                  None, v, None, x0, wdt, pos, nextrap=nextrap or nz, seed=seed)
     return _finish(w, 2.0, 60.0, 25.0, rng, tables)
 

@@ -38,6 +38,8 @@ typedef struct {
 #define IMG2D_FLAG_GENERIC 2      /* force the runtime-length kernel (testing) */
 #define IMG2D_FLAG_NO_CLUSTER 4   /* use the single-CTA kernels even where the cluster kernel applies */
 #define IMG2D_FLAG_CLUSTER_V1 8   /* first-generation cluster kernel (256 threads, fixed L) instead */
+#define IMG2D_FLAG_TABLE_FP16 16  /* operator table stored as FP16 (re, im) pairs, arithmetic FP32 */
+#define IMG2D_FLAG_TABLE_BF16 32  /* operator table stored as BF16 (re, im) pairs, arithmetic FP32 */
 /* select variant v (1-based; 0 = default) of the second-generation cluster kernel: bits 8-15 */
 #define IMG2D_FLAG_VARIANT_SHIFT 8
 #define IMG2D_FLAG_VARIANT(v) ((v) << IMG2D_FLAG_VARIANT_SHIFT)
