@@ -44,6 +44,7 @@ def parse_args():
     p.add_argument("--scale", type=float, default=1.0)
     p.add_argument("--e2e-steps", type=int, default=2)
     p.add_argument("--variant", type=int, default=0, help="cluster-kernel variant (1-based; 0 = default)")
+    p.add_argument("--no-autotune", action="store_true", help="use the plan's default kernel configuration")
     p.add_argument("--nz", type=int, default=None, help="override depth steps (profiling a reduced case)")
     p.add_argument("--nf", type=int, default=None, help="override frequency count (profiling a reduced case)")
     p.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU-baseline sample time")
@@ -246,14 +247,23 @@ def main():
     maker = synthetic.WORKLOADS[args.workload]
     over = {k: v for k, v in (("nz", args.nz), ("nf", args.nf)) if v}
     w = maker(seed=100 + rank, scale=args.scale, **over) if world > 1 else maker(scale=args.scale, **over)
-    plan = migration.Plan.for_workload(w, no_cluster=args.kernel == "single", cluster_v1=args.kernel == "cluster1",
-                                       variant=args.variant)
     om = torch.from_numpy(w.omega).to(dev)
     vel = torch.from_numpy(np.ascontiguousarray(w.velocity)).to(dev)
     tab = torch.from_numpy(w.table).to(dev)
-    plan.set_model(om, vel, w.dk, tab)
     wave0 = torch.from_numpy(w.wave).to(dev)
     shot0 = torch.from_numpy(w.shot).to(dev)
+    tune_report = None
+    if args.kernel == "auto" and args.variant == 0 and not args.no_autotune:
+        # autotuner: every candidate kernel configuration on the first depth steps of this workload
+        best, rows = migration.autotune(w.ns, w.nextrap, w.nz, w.nx, w.nf, w.nt, w.M, w.nk, w.dk, om, vel, tab,
+                                        wave0, shot0, shot_x0=w.shot_x0, shot_nx=w.shot_nx, trial_depths=8)
+        tune_report = {"trial_depths": 8, "picked": rows[0][1],
+                       "ms": {n: round(t, 3) for t, n, _ in rows}}
+        plan = migration.Plan.for_workload(w, **best)
+    else:
+        plan = migration.Plan.for_workload(w, no_cluster=args.kernel == "single",
+                                           cluster_v1=args.kernel == "cluster1", variant=args.variant)
+    plan.set_model(om, vel, w.dk, tab)
     wave = torch.empty_like(wave0)
     shot = torch.empty_like(shot0)
     image = torch.zeros((w.nz, w.nx), dtype=torch.float32, device=dev)
@@ -317,6 +327,8 @@ def main():
         extra["roofline"] = roof
         extra["roofline_hbm"] = roof_hbm
         extra["kernel_config"] = describe
+        if tune_report:
+            extra["autotune"] = tune_report
 
     # end to end through the host C entry point, pinned host buffers, copies inside the timed region
     if rank == 0 and not args.no_e2e:
@@ -374,9 +386,18 @@ def main():
         a1.synchronize()
         nsec = a0.elapsed_time(a1) / 1e3
         npts = sub.points()
+        # the same launch sequence captured once as a CUDA graph and replayed
+        g = migration.GraphedExecution(nplan, sw, ss, si, naive=True)
+        a0.record()
+        g.replay()
+        a1.record()
+        a1.synchronize()
+        gsec = a0.elapsed_time(a1) / 1e3
         extra["plain_naive"] = {"value": npts / nsec, "unit": UNIT, "launches": ns_s * nf_s * (w.nextrap + 1),
                                 "sample": f"1 shot x {nf_s} frequencies x {w.nextrap} depths, one launch per "
-                                          "(shot, w, z)", "batched_over_naive": value / world / (npts / nsec)}
+                                          "(shot, w, z)", "batched_over_naive": value / world / (npts / nsec),
+                                "graph_replay_value": npts / gsec}
+        del g
         nplan.close()
 
     if rank == 0 and not args.no_cpu_baseline and world == 1:

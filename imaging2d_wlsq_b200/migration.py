@@ -132,3 +132,81 @@ class Plan:
         buf = ctypes.create_string_buffer(512)
         check(lib().img2d_plan_describe(self._h, buf, 512))
         return json.loads(buf.value.decode())
+
+
+# ---------------------------------------------------------------------------------------------
+# Autotuning and graph capture
+# ---------------------------------------------------------------------------------------------
+
+# Candidate kernel configurations, as Plan keyword arguments.  cluster2 variants differ in warps per
+# CTA (positions per CTA), operator-pair prefetch depth, L1 row prefetch and packed arithmetic.
+CANDIDATES = [("cluster2/v%d" % v, {"variant": v}) for v in range(1, 8)] + \
+             [("cluster1", {"cluster_v1": True}), ("single-cta", {"no_cluster": True})]
+
+
+def autotune(ns, nextrap, nz, nx, nf, nt, M, nk, dk, omega, velocity, table, wave, shot, shot_x0=None,
+             shot_nx=None, trial_depths=12, repeats=2, candidates=None):
+    """Pick the fastest kernel configuration for this geometry.
+
+    Each candidate runs the first `trial_depths` depth steps of the migration (every shot and
+    frequency) on copies of the device wavefields; its kernel time is the best of `repeats` runs
+    after one warm-up.  Candidates that do not apply to the geometry, or that resolve to the same
+    kernel configuration as an earlier one, are skipped.  Returns (best Plan kwargs, table of
+    (milliseconds, name, describe()) sorted fastest first)."""
+    import torch
+    from ._lib import LibraryError
+    trial = max(1, min(nextrap, trial_depths))
+    seen = set()
+    table_rows = []
+    for name, kw in (candidates or CANDIDATES):
+        try:
+            plan = Plan(ns, trial, nz, nx, nf, nt, M, nk, shot_x0, shot_nx, **kw)
+        except LibraryError:
+            continue
+        d = plan.describe()
+        key = (d["kernel"], d["variant"], d["cluster"], d["G"], d["block"])
+        if key in seen:
+            plan.close()
+            continue
+        seen.add(key)
+        plan.set_model(omega, velocity, dk, table)
+        w2, s2 = wave.clone(), shot.clone()
+        img = torch.zeros((nz, nx), dtype=torch.float32, device=wave.device)
+        times = []
+        for _ in range(repeats + 1):
+            plan.execute(w2, s2, img)
+            times.append(plan.kernel_ms())
+        table_rows.append((min(times[1:]), name, d, kw))
+        plan.close()
+    if not table_rows:
+        raise RuntimeError("no kernel configuration applies to this geometry")
+    table_rows.sort(key=lambda r: r[0])
+    return table_rows[0][3], [(t, n, d) for t, n, d, _ in table_rows]
+
+
+def tuned_plan(w, omega, velocity, table, wave, shot, **kw):
+    """Plan for synthetic.Workload-like `w` with the configuration autotune() picks."""
+    best, report = autotune(w.ns, w.nextrap, w.nz, w.nx, w.nf, w.nt, w.M, w.nk, w.dk, omega, velocity, table, wave,
+                            shot, shot_x0=w.shot_x0, shot_nx=w.shot_nx, **kw)
+    return Plan.for_workload(w, **best), report
+
+
+class GraphedExecution:
+    """One migration of a plan (or its naive per-(shot, w, z) launch sequence) captured as a CUDA
+    graph on fixed device buffers; replay() re-runs it with whatever the buffers hold."""
+
+    def __init__(self, plan, wave, shot, image, naive=False):
+        import torch
+        self.plan, self.naive = plan, naive
+        self.buffers = (wave, shot, image)
+        run = plan.execute_naive if naive else plan.execute
+        # one eager run creates the plan's lazily made resources (events, scratch) before capture
+        run(wave, shot, image)
+        torch.cuda.synchronize()
+        self.graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(self.graph):
+            run(wave, shot, image)
+        torch.cuda.synchronize()
+
+    def replay(self):
+        self.graph.replay()

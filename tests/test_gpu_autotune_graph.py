@@ -1,0 +1,59 @@
+"""Autotuner and CUDA-graph execution of the migration (GPU)."""
+import numpy as np
+import pytest
+
+from imaging2d_wlsq_b200 import migration, synthetic
+from oracle import oracle
+from tests.conftest import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+
+def _dev(w):
+    import torch
+    dev = torch.device("cuda")
+    return (torch.from_numpy(w.omega).to(dev), torch.from_numpy(np.ascontiguousarray(w.velocity)).to(dev),
+            torch.from_numpy(w.table).to(dev), torch.from_numpy(w.wave.copy()).to(dev),
+            torch.from_numpy(w.shot.copy()).to(dev))
+
+
+def test_autotune_picks_a_configuration_that_matches_the_oracle():
+    import torch
+    w = synthetic.batched_uneven(nx=1200, nz=10, nf=6, ns=40)
+    om, vel, tab, wave, shot = _dev(w)
+    plan, report = migration.tuned_plan(w, om, vel, tab, wave, shot, trial_depths=4, repeats=1)
+    assert len(report) >= 3 and report[0][0] <= report[-1][0]
+    names = [r[1] for r in report]
+    assert "single-cta" in names and any(n.startswith("cluster2") for n in names)
+    plan.set_model(om, vel, w.dk, tab)
+    img = torch.zeros((w.nz, w.nx), dtype=torch.float32, device=wave.device)
+    plan.execute(wave, shot, img)
+    torch.cuda.synchronize()
+    stack, _, wo, so = oracle.migrate_workload_f64(w)
+    assert rel_l2(img.cpu().numpy(), stack) <= 1e-5
+    assert rel_l2(wave.cpu().numpy(), wo) <= 1e-5
+    plan.close()
+
+
+@pytest.mark.parametrize("naive", [False, True])
+def test_graph_replay_matches_eager(naive):
+    import torch
+    w = synthetic.plain_medium(nx=256, nz=8, nf=3, ns=16)
+    om, vel, tab, wave, shot = _dev(w)
+    plan = migration.Plan.for_workload(w)
+    plan.set_model(om, vel, w.dk, tab)
+    wave0, shot0 = wave.clone(), shot.clone()
+    img = torch.zeros((w.nz, w.nx), dtype=torch.float32, device=wave.device)
+    g = migration.GraphedExecution(plan, wave, shot, img, naive=naive)
+    outs = []
+    for _ in range(2):
+        wave.copy_(wave0)
+        shot.copy_(shot0)
+        g.replay()
+        torch.cuda.synchronize()
+        outs.append((img.cpu().numpy().copy(), wave.cpu().numpy().copy()))
+    stack, _, wo, _ = oracle.migrate_workload_f64(w)
+    for im, wv in outs:
+        assert rel_l2(im, stack) <= 1e-5
+        assert rel_l2(wv, wo) <= 1e-5
+    plan.close()
