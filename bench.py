@@ -51,6 +51,8 @@ def parse_args():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-naive", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-lsm", action="store_true", help="skip the demigration / least-squares migration leg")
+    p.add_argument("--lsm-iters", type=int, default=10)
     p.add_argument("--accuracy", action="store_true",
                    help="CPU leg also checks rel-L2 against the FP64 checker on a sub-volume")
     p.add_argument("--kernel", default="auto", choices=["auto", "cluster1", "single"],
@@ -216,6 +218,61 @@ def run_reference_impl(args):
     }
     print(json.dumps(line), flush=True)
     return 0
+
+
+def lsm_leg(dev, iters):
+    """Demigration (adjoint) and least-squares migration on the lsm configuration: nz=500, nx=1024,
+    nf=256 (2-40 Hz), 31 taps, 64 full-aperture shots, 0.5% sparse reflectivity; observed data
+    synthesised by the demigration kernel."""
+    import torch
+    from imaging2d_wlsq_b200 import lsm, synthetic
+    w = synthetic.lsm()
+    op = lsm.MigrationOperator.for_workload(w, device=dev)
+    m_true = torch.from_numpy(w.reflectivity[:w.nextrap]).to(dev)
+    for _ in range(3):
+        d_obs = op.demigrate(m_true)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    d_obs = op.demigrate(m_true)
+    e1.record()
+    e1.synchronize()
+    t_dem = e0.elapsed_time(e1) / 1e3
+    kms_dem = op.plan.kernel_ms()
+    d_obs = d_obs.clone()
+    e0.record()
+    op.migrate(d_obs)
+    e1.record()
+    e1.synchronize()
+    t_mig = e0.elapsed_time(e1) / 1e3
+    pts = w.points()
+    dots = [lsm.dot_product_test(op, seed=sd) for sd in range(3)]
+    rng = np.random.default_rng(5)
+    pts16 = [(int(rng.integers(0, w.nextrap)), int(rng.integers(0, w.nx))) for _ in range(16)]
+    ga, fd = lsm.finite_difference_check(op, torch.zeros_like(m_true), d_obs, pts16, h=1.0)
+    _, hist = lsm.lsm_cg(op, d_obs, niter=iters)
+    _, hist2 = lsm.cgls(op, d_obs, niter=iters)
+    out = {
+        "workload": f"lsm: nz={w.nz} nx={w.nx} nf={w.nf} taps={w.L} nk={w.nk} ns={w.ns} full aperture, "
+                    "reflectivity 0.5% spikes * [1,2,1]/4 (z, x), d_obs = F* m_true",
+        "demigration": {"value": pts / t_dem, "unit": UNIT, "seconds": t_dem, "kernel_ms": kms_dem,
+                        "kernel_config": op.plan.describe_demigration()},
+        "migration": {"value": pts / t_mig, "unit": UNIT, "seconds": t_mig},
+        "dot_product": {"rel": [d[2] for d in dots], "rel_norms": [d[3] for d in dots],
+                        "seeds": 3, "vectors": "Gaussian d (complex) and m",
+                        "rel_def": "|<Fd,m> - <d,F*m>| / max(|<Fd,m>|, |<d,F*m>|)",
+                        "rel_norms_def": "|<Fd,m> - <d,F*m>| / (||Fd|| ||m||)"},
+        "fd_gradient": {"points": 16, "h": 1.0, "max_abs_err_over_max_grad": float(np.max(np.abs(ga - fd)) /
+                                                                                    np.abs(ga).max())},
+        "cg_autograd": {"iterations": iters, "residual_ratio": hist[-1][1] / hist[0][1],
+                        "s_per_iteration": hist[-1][2] / iters,
+                        "per_iteration": "1 demigration + 1 migration (autograd backward) + 1 demigration (step)"},
+        "cgls": {"iterations": iters, "residual_ratio": hist2[-1][1] / hist2[0][1],
+                 "s_per_iteration": hist2[-1][2] / iters, "per_iteration": "1 demigration + 1 migration"},
+    }
+    op.plan.close()
+    return out
 
 
 def workload_config(w, args):
@@ -428,6 +485,12 @@ def main():
                                  "sub_volume": f"first {sub_n} depth steps, all shots and frequencies",
                                  "reference": "FP64 CPU checker"}
             plan_a.close()
+
+    if rank == 0 and world == 1 and not args.no_lsm:
+        try:
+            extra["lsm"] = lsm_leg(dev, args.lsm_iters)
+        except Exception as ex:
+            extra["lsm"] = {"error": f"{type(ex).__name__}: {ex}"}
 
     if rank == 0:
         line = {

@@ -92,6 +92,10 @@ def load():
     lib.img2d_measure_fp32_peak.argtypes = [POINTER(c_double)]
     lib.img2d_migrate_compact_noalloc.restype = c_int
     lib.img2d_migrate_compact_noalloc.argtypes = [c_int] * 8 + [c_double] + [c_void_p] * 9
+    lib.img2d_plan_demigrate.restype = c_int
+    lib.img2d_plan_demigrate.argtypes = [c_void_p] * 4 + [c_int, c_void_p]
+    lib.img2d_plan_describe_demigration.restype = c_int
+    lib.img2d_plan_describe_demigration.argtypes = [c_void_p, c_char_p, c_int]
     lib.img2d_plan_destroy.restype = None
     lib.img2d_plan_destroy.argtypes = [c_void_p]
     return lib

@@ -12,6 +12,7 @@
 #include "wlsq_kernels.cuh"
 #include "wlsq_cluster.cuh"
 #include "wlsq_cluster2.cuh"
+#include "wlsq_adjoint.cuh"
 
 namespace img2d {
 
@@ -113,6 +114,37 @@ static const Cluster2Variant kCluster2[] = {
 };
 constexpr int kCluster2Default = 0;
 constexpr int kNumCluster2 = (int)(sizeof(kCluster2) / sizeof(kCluster2[0]));
+
+// Demigration kernels: G lane slots per item, compile-time operator length (0 = runtime length).
+constexpr int kAdjWarps = 16;
+typedef void (*DemigFn)(DemigrateArgs);
+struct DemigKernel {
+    int G, L;
+    DemigFn fn;
+};
+#define IMG2D_DEMIG(G, L) {G, L, demigrate_kernel<G, L, kAdjWarps>}
+#define IMG2D_DEMIG_G(G) IMG2D_DEMIG(G, 0), IMG2D_DEMIG(G, 25), IMG2D_DEMIG(G, 31), IMG2D_DEMIG(G, 35), IMG2D_DEMIG(G, 55)
+static const DemigKernel kDemig[] = {IMG2D_DEMIG_G(2), IMG2D_DEMIG_G(4), IMG2D_DEMIG_G(8)};
+
+static DemigFn find_demig(int G, int L)
+{
+    DemigFn generic = nullptr;
+    for (const auto &k : kDemig) {
+        if (k.G != G) continue;
+        if (k.L == L) return k.fn;
+        if (k.L == 0) generic = k.fn;
+    }
+    return generic;
+}
+
+// Shared memory of the demigration kernel: one complex wavefield per slot, ping-pong.
+static size_t demig_smem_bytes(int G, int W, int M)
+{
+    const int X = 8;
+    const int Mp = ((M + X - 1) / X) * X;
+    const int Wp = ((W + X - 1) / X) * X;
+    return 2 * (size_t)((Mp + Wp + Mp) / X * (X + 1)) * G * sizeof(float2);
+}
 
 static const ClusterKernel *find_cluster(int L)
 {
@@ -266,6 +298,14 @@ struct img2d_plan {
     bool timing = true;               // record events around the migration kernel
     img2d::DevBuf items, groups, segs, owner, shot_off, idx, tabF, tabB, tab16buf, partial, comp, counter, naive_buf;
     // dense tables (drop-in ABI) are owned by the caller of run_dense
+    // lane-slot packing: shots of each slot, slots ordered by extent, right end of each slot
+    std::vector<std::vector<int>> slots;
+    std::vector<int> slot_order, slot_end;
+    // demigration (adjoint) launch state, built on its first call
+    int adj_G = 0, adj_grid = 0, adj_items_n = 0, adj_wmax = 0, adj_block = 0, adj_slab = 0, adj_nslab = 0;
+    size_t adj_smem = 0;
+    void (*adj_fn)(img2d::DemigrateArgs) = nullptr;
+    img2d::DevBuf adj_items, adj_groups, adj_segs, adj_owner, adj_work, adj_counter;
 };
 
 namespace img2d {
@@ -289,6 +329,45 @@ static size_t smem_bytes(int G, int W, int M, int X)
     const int npos = Mp + Wp + Mp;
     const size_t nslot = (size_t)npos / X * (X + 1);
     return 2 * nslot * G * sizeof(float4);
+}
+
+// Slots of similar extent form groups of G that share a work item; returns the widest group.
+static int pack_groups(const img2d_plan *p, int G, std::vector<GroupDesc> &groups, std::vector<int4> &segs,
+                       std::vector<int16_t> &owner)
+{
+    groups.clear();
+    segs.clear();
+    owner.clear();
+    int widest = 0;
+    const std::vector<int> &sorder = p->slot_order;
+    for (size_t g0 = 0; g0 < sorder.size(); g0 += G) {
+        const int n = (int)std::min<size_t>(G, sorder.size() - g0);
+        int u0 = p->nx, u1 = 0;
+        for (int k = 0; k < n; ++k) {
+            const int i = sorder[g0 + k];
+            u0 = std::min(u0, p->x0[p->slots[i].front()]);
+            u1 = std::max(u1, p->slot_end[i]);
+        }
+        GroupDesc gd{};
+        gd.seg_begin = (int)segs.size();
+        gd.u0 = u0;
+        gd.W = u1 - u0;
+        gd.nslots = n;
+        gd.owner_stride = (gd.W + 7) / 8 * 8;
+        gd.owner_off = (long long)owner.size();
+        owner.resize(owner.size() + (size_t)n * gd.owner_stride, (int16_t)-1);
+        for (int k = 0; k < n; ++k) {
+            for (int s : p->slots[sorder[g0 + k]]) {
+                segs.push_back(make_int4(s, k, p->x0[s], p->w[s]));
+                int16_t *row = owner.data() + gd.owner_off + (size_t)k * gd.owner_stride;
+                for (int x = p->x0[s]; x < p->x0[s] + p->w[s]; ++x) row[x - u0] = (int16_t)s;
+            }
+        }
+        gd.nseg = (int)segs.size() - gd.seg_begin;
+        groups.push_back(gd);
+        widest = std::max(widest, gd.W);
+    }
+    return widest;
 }
 
 static int build_plan(img2d_plan *p, int ns, int nextrap, int nz, int nx, int nf, int nt, int M,
@@ -356,45 +435,14 @@ static int build_plan(img2d_plan *p, int ns, int nextrap, int nz, int nx, int nf
         return slot_end[a] < slot_end[b];
     });
     p->n_slots = (int)slots.size();
+    p->slots = slots;
+    p->slot_order = sorder;
+    p->slot_end = slot_end;
 
-    // Slots of similar extent form groups of G that share a work item.
     std::vector<GroupDesc> groups;
     std::vector<int4> segs;
     std::vector<int16_t> owner;
-    auto make_groups = [&](int G) {
-        groups.clear();
-        segs.clear();
-        owner.clear();
-        int widest = 0;
-        for (size_t g0 = 0; g0 < sorder.size(); g0 += G) {
-            const int n = (int)std::min<size_t>(G, sorder.size() - g0);
-            int u0 = nx, u1 = 0;
-            for (int k = 0; k < n; ++k) {
-                const int i = sorder[g0 + k];
-                u0 = std::min(u0, ext0(i));
-                u1 = std::max(u1, slot_end[i]);
-            }
-            GroupDesc gd{};
-            gd.seg_begin = (int)segs.size();
-            gd.u0 = u0;
-            gd.W = u1 - u0;
-            gd.nslots = n;
-            gd.owner_stride = (gd.W + 7) / 8 * 8;
-            gd.owner_off = (long long)owner.size();
-            owner.resize(owner.size() + (size_t)n * gd.owner_stride, (int16_t)-1);
-            for (int k = 0; k < n; ++k) {
-                for (int s : slots[sorder[g0 + k]]) {
-                    segs.push_back(make_int4(s, k, p->x0[s], p->w[s]));
-                    int16_t *row = owner.data() + gd.owner_off + (size_t)k * gd.owner_stride;
-                    for (int x = p->x0[s]; x < p->x0[s] + p->w[s]; ++x) row[x - u0] = (int16_t)s;
-                }
-            }
-            gd.nseg = (int)segs.size() - gd.seg_begin;
-            groups.push_back(gd);
-            widest = std::max(widest, gd.W);
-        }
-        return widest;
-    };
+    auto make_groups = [&](int G) { return pack_groups(p, G, groups, segs, owner); };
 
     // Kernel choice.  The cluster kernel (16 slots per item, 256 positions per CTA, up to 8 CTAs
     // per cluster) when the operator length has an instance, there are enough slots to fill it
@@ -654,6 +702,69 @@ static int set_model(img2d_plan *p, const double *d_omega, const double *d_vel, 
     return IMG2D_OK;
 }
 
+// Launch state of the demigration: its own slot groups (one complex wavefield per slot, so up to
+// 8 slots fit beside the halos), items, and the per-CTA checkpoint / slab / save planes.
+static int demig_prepare(img2d_plan *p, int slab)
+{
+    if (slab <= 0) slab = 8;
+    slab = std::min(slab, p->nextrap);
+    const int nslab = (p->nextrap + slab - 1) / slab;
+    if (p->adj_fn && p->adj_slab == slab) return IMG2D_OK;
+    int dev = 0, smem_optin = 0, nsm = 0;
+    IMG2D_CUDA(cudaGetDevice(&dev));
+    IMG2D_CUDA(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    IMG2D_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    const int static_reserve = 1024;
+    std::vector<GroupDesc> groups;
+    std::vector<int4> segs;
+    std::vector<int16_t> owner;
+    int G = 8, widest = 0;
+    for (;; G >>= 1) {
+        widest = pack_groups(p, G, groups, segs, owner);
+        if (demig_smem_bytes(G, widest, p->M) + static_reserve <= (size_t)smem_optin) break;
+        if (G == 2) return fail(IMG2D_EINVAL, "aperture too wide for the demigration kernel's shared memory");
+    }
+    // fewer slots than lanes: smaller groups leave fewer idle lanes
+    while (G > 2 && (int)p->slot_order.size() <= G / 2) G >>= 1;
+    widest = pack_groups(p, G, groups, segs, owner);
+    DemigFn fn = find_demig(G, p->L);
+    if (!fn) return fail(IMG2D_EINVAL, "no demigration kernel for this configuration");
+    const size_t smem = demig_smem_bytes(G, widest, p->M);
+    IMG2D_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int bps = 0;
+    IMG2D_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, fn, kAdjWarps * 32, smem));
+    if (bps <= 0) return fail(IMG2D_ECUDA, "demigration kernel does not fit on an SM");
+    std::vector<int2> items;
+    std::vector<int> gorder(groups.size());
+    std::iota(gorder.begin(), gorder.end(), 0);
+    std::stable_sort(gorder.begin(), gorder.end(), [&](int a, int b) { return groups[a].W > groups[b].W; });
+    for (int g : gorder)
+        for (int j = 0; j < p->nf; ++j) items.push_back(make_int2(g, j));
+    const int grid = (int)std::min<size_t>(items.size(), (size_t)nsm * bps);
+    const long long work_cta = (long long)(nslab + slab + 1) * widest * G;
+    int rc;
+    if ((rc = p->adj_items.ensure(items.size() * sizeof(int2)))) return rc;
+    if ((rc = p->adj_groups.ensure(groups.size() * sizeof(GroupDesc)))) return rc;
+    if ((rc = p->adj_segs.ensure(segs.size() * sizeof(int4)))) return rc;
+    if ((rc = p->adj_owner.ensure(owner.size() * sizeof(int16_t)))) return rc;
+    if ((rc = p->adj_counter.ensure(sizeof(int)))) return rc;
+    if ((rc = p->adj_work.ensure((size_t)grid * work_cta * sizeof(float2)))) return rc;
+    IMG2D_CUDA(cudaMemcpy(p->adj_items.p, items.data(), items.size() * sizeof(int2), cudaMemcpyHostToDevice));
+    IMG2D_CUDA(cudaMemcpy(p->adj_groups.p, groups.data(), groups.size() * sizeof(GroupDesc), cudaMemcpyHostToDevice));
+    IMG2D_CUDA(cudaMemcpy(p->adj_segs.p, segs.data(), segs.size() * sizeof(int4), cudaMemcpyHostToDevice));
+    IMG2D_CUDA(cudaMemcpy(p->adj_owner.p, owner.data(), owner.size() * sizeof(int16_t), cudaMemcpyHostToDevice));
+    p->adj_G = G;
+    p->adj_grid = grid;
+    p->adj_items_n = (int)items.size();
+    p->adj_wmax = widest;
+    p->adj_block = kAdjWarps * 32;
+    p->adj_slab = slab;
+    p->adj_nslab = nslab;
+    p->adj_smem = smem;
+    p->adj_fn = fn;
+    return IMG2D_OK;
+}
+
 // Scoped device allocation for the host entry points.
 struct Scratch {
     std::vector<void *> ptrs;
@@ -814,6 +925,68 @@ int img2d_plan_execute(img2d_plan *p, img2d_c64 *d_wave, img2d_c64 *d_shot, floa
     return launch(p, a, d_image, d_image_shots, (long long)p->nz * p->nx, (cudaStream_t)stream);
 }
 
+int img2d_plan_demigrate(img2d_plan *p, const float *d_refl, const img2d_c64 *d_wave, img2d_c64 *d_data,
+                         int slab_depth, void *stream)
+{
+    if (!p) return fail(IMG2D_EINVAL, "plan is NULL");
+    if (!d_refl || !d_wave || !d_data) return fail(IMG2D_EINVAL, "null device pointer");
+    if ((const void *)d_wave == (const void *)d_data) return fail(IMG2D_EINVAL, "data must not alias wave");
+    if (p->mode != OP_CONJ) return fail(IMG2D_EINVAL, "demigration supports the single-table mode only");
+    int rc;
+    if ((rc = demig_prepare(p, slab_depth))) return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    DemigrateArgs a{};
+    a.nextrap = p->nextrap;
+    a.nx = p->nx;
+    a.M = p->M;
+    a.tab_stride = p->tab_stride;
+    a.n_items = p->adj_items_n;
+    a.slab = p->adj_slab;
+    a.nslab = p->adj_nslab;
+    a.items = p->adj_items.as<int2>();
+    a.groups = p->adj_groups.as<GroupDesc>();
+    a.segs = p->adj_segs.as<int4>();
+    a.owner = p->adj_owner.as<int16_t>();
+    a.shot_off = p->shot_off.as<long long>();
+    a.tab = p->tabF.as<cpx>();
+    a.idx = p->idx.as<uint16_t>();
+    a.idx_jstride = (long long)p->nextrap * p->idx_lstride;
+    a.idx_lstride = p->idx_lstride;
+    a.wave = (const cpx *)d_wave;
+    a.refl = d_refl;
+    a.data = (cpx *)d_data;
+    a.work = p->adj_work.as<float2>();
+    a.work_cta = (long long)(p->adj_nslab + p->adj_slab + 1) * p->adj_wmax * p->adj_G;
+    a.wmax = p->adj_wmax;
+    a.counter = p->adj_counter.as<int>();
+    IMG2D_CUDA(cudaMemsetAsync(p->adj_counter.p, 0, sizeof(int), st));
+    if (p->timing && !p->ev0) {
+        IMG2D_CUDA(cudaEventCreate(&p->ev0));
+        IMG2D_CUDA(cudaEventCreate(&p->ev1));
+    }
+    if (p->timing) IMG2D_CUDA(cudaEventRecord(p->ev0, st));
+    p->adj_fn<<<p->adj_grid, p->adj_block, p->adj_smem, st>>>(a);
+    IMG2D_CUDA(cudaGetLastError());
+    if (p->timing) {
+        IMG2D_CUDA(cudaEventRecord(p->ev1, st));
+        p->ev_recorded = true;
+    }
+    return IMG2D_OK;
+}
+
+int img2d_plan_describe_demigration(const img2d_plan *p, char *buf, int buflen)
+{
+    if (!p || !buf || buflen <= 0) return fail(IMG2D_EINVAL, "bad describe arguments");
+    if (!p->adj_fn) return fail(IMG2D_EINVAL, "no demigration has run on this plan yet");
+    snprintf(buf, buflen,
+             "{\"kernel\": \"demigrate\", \"G\": %d, \"X\": 8, \"L\": %d, \"grid\": %d, \"block\": %d, "
+             "\"smem\": %zu, \"items\": %d, \"max_union_width\": %d, \"slab\": %d, \"slabs\": %d, "
+             "\"workspace_bytes\": %zu}",
+             p->adj_G, p->L, p->adj_grid, p->adj_block, p->adj_smem, p->adj_items_n, p->adj_wmax, p->adj_slab,
+             p->adj_nslab, p->adj_work.bytes);
+    return IMG2D_OK;
+}
+
 long long img2d_plan_shot_offset(const img2d_plan *p, int s)
 {
     if (!p || s < 0 || s >= p->ns) return -1;
@@ -827,7 +1000,8 @@ size_t img2d_plan_workspace_bytes(const img2d_plan *p)
     if (!p) return 0;
     return p->items.bytes + p->groups.bytes + p->segs.bytes + p->owner.bytes + p->shot_off.bytes +
            p->idx.bytes + p->tabF.bytes + p->tabB.bytes + p->tab16buf.bytes + p->partial.bytes + p->comp.bytes + p->counter.bytes +
-           p->naive_buf.bytes;
+           p->naive_buf.bytes + p->adj_items.bytes + p->adj_groups.bytes + p->adj_segs.bytes + p->adj_owner.bytes +
+           p->adj_work.bytes + p->adj_counter.bytes;
 }
 
 int img2d_plan_describe(const img2d_plan *p, char *buf, int buflen)

@@ -1,0 +1,251 @@
+"""Least-squares migration on the B200 kernels: the migration operator, its adjoint (demigration),
+torch.autograd bindings, and conjugate-gradient solvers.
+
+No counterpart in the reference, which only migrates (main.py:136-186 calls the extrapolation
+libraries once and stacks the per-shot images).  The forward map here is the reference's
+migration, cpp_src/extrapolation_cpu.cpp:39-89, seen as a linear map of the receiver spectra d for
+a fixed source:
+
+    F d = image,  image[l, x] = Re sum_{shots, w} S_{l+1}[x] conj(R_{l+1}[x]),  R_0 = d
+
+(Plan.execute), and the modelling operator of least-squares migration is its adjoint
+
+    F* m = demigrated receiver spectra of the reflectivity m      (Plan.demigrate)
+
+with <F d, m> = Re sum d conj(F* m).  Least-squares migration solves min_m 1/2 ||F* m - d_obs||^2.
+
+Data live on the device in the packed wavefield layout of the plan (complex64, per shot nt rows of
+that shot's aperture); images are float32 (nextrap, nx).
+"""
+import time
+
+import numpy as np
+
+from .migration import Plan
+
+
+class MigrationOperator:
+    """F (migrate) and F* (demigrate) for one survey geometry, model and source.
+
+    plan    a migration.Plan whose model is set (single-table mode)
+    wave    device complex64 source spectra in the plan's packed layout; kept, never modified
+    """
+
+    def __init__(self, plan, wave, slab_depth=0):
+        import torch
+        self.plan = plan
+        self.wave = wave
+        self.slab_depth = slab_depth
+        self.nextrap, self.nx = plan.nextrap, plan.nx
+        self.device = wave.device
+        self._src = torch.empty_like(wave)
+        self._rec = torch.empty_like(wave)
+
+    @classmethod
+    def for_workload(cls, w, device=None, slab_depth=0, **plan_kw):
+        import torch
+        dev = device or torch.device("cuda")
+        plan = Plan.for_workload(w, **plan_kw)
+        plan.set_model(torch.from_numpy(w.omega).to(dev), torch.from_numpy(np.ascontiguousarray(w.velocity)).to(dev),
+                       w.dk, torch.from_numpy(w.table).to(dev))
+        return cls(plan, torch.from_numpy(w.wave).to(dev), slab_depth=slab_depth)
+
+    def zeros_data(self):
+        import torch
+        return torch.zeros_like(self.wave)
+
+    def zeros_image(self):
+        import torch
+        return torch.zeros((self.nextrap, self.nx), dtype=torch.float32, device=self.device)
+
+    def migrate(self, data, image=None):
+        """F d: stacked image (nextrap, nx) of the receiver spectra `data` (not modified)."""
+        import torch
+        image = self.zeros_image() if image is None else image
+        self._src.copy_(self.wave)
+        self._rec.copy_(data)
+        self.plan.execute(self._src, self._rec, image, stream=torch.cuda.current_stream(self.device))
+        return image
+
+    def demigrate(self, refl, data=None):
+        """F* m: receiver spectra (packed layout) of the reflectivity `refl` (nextrap, nx)."""
+        import torch
+        data = self.zeros_data() if data is None else data
+        self.plan.demigrate(refl.contiguous(), self.wave, data, slab_depth=self.slab_depth,
+                            stream=torch.cuda.current_stream(self.device))
+        return data
+
+
+def _functions():
+    import torch
+
+    class Demigrate(torch.autograd.Function):
+        """refl (real) -> data (complex).  Backward: the gradient of a real loss with respect to
+        refl is F applied to the complex gradient of the data (torch's convention
+        dL/dRe + i dL/dIm)."""
+
+        @staticmethod
+        def forward(ctx, refl, op):
+            ctx.op = op
+            return op.demigrate(refl)
+
+        @staticmethod
+        def backward(ctx, grad_data):
+            return ctx.op.migrate(grad_data.contiguous()), None
+
+    class Migrate(torch.autograd.Function):
+        """data (complex) -> image (real).  Backward: F* of the image gradient."""
+
+        @staticmethod
+        def forward(ctx, data, op):
+            ctx.op = op
+            return op.migrate(data)
+
+        @staticmethod
+        def backward(ctx, grad_image):
+            return ctx.op.demigrate(grad_image.contiguous()), None
+
+    return Demigrate, Migrate
+
+
+_FN = None
+
+
+def _fn():
+    global _FN
+    if _FN is None:
+        _FN = _functions()
+    return _FN
+
+
+def demigrate(refl, op):
+    """Differentiable F* refl."""
+    return _fn()[0].apply(refl, op)
+
+
+def migrate(data, op):
+    """Differentiable F data."""
+    return _fn()[1].apply(data, op)
+
+
+def _dot_r(a, b):
+    """Real inner product in float64: sum a b for real tensors, Re sum a conj(b) for complex."""
+    import torch
+    if a.is_complex():
+        return float(torch.sum(a.real.double() * b.real.double() + a.imag.double() * b.imag.double()))
+    return float(torch.sum(a.double() * b.double()))
+
+
+def dot_product_test(op, seed=0, data=None, refl=None):
+    """<F d, m> against Re sum d conj(F* m) for seeded Gaussian d and m.  Returns
+    (lhs, rhs, rel, rel_norms) with rel = |lhs - rhs| / max(|lhs|, |rhs|) and
+    rel_norms = |lhs - rhs| / (||F d|| ||m||).  Independent random vectors make lhs a sum of
+    terms of both signs, so rel grows as lhs happens to cancel; rel_norms is the same difference on
+    the Cauchy-Schwarz scale, where a wrong adjoint shows up near 1/sqrt(size of the image)."""
+    import torch
+    g = torch.Generator(device=op.device).manual_seed(seed)
+    if data is None:
+        data = torch.randn(op.wave.shape, dtype=torch.complex64, device=op.device, generator=g)
+    if refl is None:
+        refl = torch.randn((op.nextrap, op.nx), dtype=torch.float32, device=op.device, generator=g)
+    img = op.migrate(data)
+    lhs = _dot_r(img, refl)
+    rhs = _dot_r(data, op.demigrate(refl))
+    scale = np.sqrt(_dot_r(img, img) * _dot_r(refl, refl))
+    return lhs, rhs, abs(lhs - rhs) / max(abs(lhs), abs(rhs)), abs(lhs - rhs) / scale
+
+
+def misfit(op, refl, d_obs):
+    """J(m) = 1/2 ||F* m - d_obs||^2 in float64."""
+    r = op.demigrate(refl) - d_obs
+    return 0.5 * _dot_r(r, r)
+
+
+def finite_difference_check(op, refl, d_obs, points, h):
+    """Gradient of J at `refl` by autograd (through Demigrate) against central differences
+    (J(m + h e_i) - J(m - h e_i)) / 2h at the image points `points` [(l, x), ...].  J is quadratic,
+    so the central difference is exact up to rounding for any h.  Returns (autograd, fd) arrays."""
+    import torch
+    m = refl.detach().clone().requires_grad_(True)
+    r = demigrate(m, op) - d_obs
+    loss = 0.5 * (r.real.double().pow(2).sum() + r.imag.double().pow(2).sum())
+    loss.backward()
+    grad = m.grad.detach()
+    ga, fd = [], []
+    with torch.no_grad():
+        for (l, x) in points:
+            mp = refl.detach().clone()
+            mp[l, x] += h
+            jp = misfit(op, mp, d_obs)
+            mp[l, x] -= 2 * h
+            jm = misfit(op, mp, d_obs)
+            ga.append(float(grad[l, x]))
+            fd.append((jp - jm) / (2 * h))
+    return np.array(ga), np.array(fd)
+
+
+def lsm_cg(op, d_obs, niter, refl0=None, callback=None):
+    """Least-squares migration by conjugate gradients on 1/2 ||F* m - d_obs||^2 with the gradient
+    from torch autograd: each iteration evaluates the misfit through Demigrate, back-propagates
+    (one migration), takes the Fletcher-Reeves direction and the exact step along it (one more
+    demigration).  Returns (m, history) with history rows (iteration, ||r||, seconds)."""
+    import torch
+    m = op.zeros_image() if refl0 is None else refl0.detach().clone()
+    p = None
+    gg_prev = None
+    hist = []
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for it in range(niter + 1):
+        m.requires_grad_(True)
+        r = demigrate(m, op) - d_obs
+        rr = r.real.double().pow(2).sum() + r.imag.double().pow(2).sum()
+        loss = 0.5 * rr
+        rnorm = float(rr.detach().sqrt())
+        if it == niter:
+            torch.cuda.synchronize()
+            hist.append((it, rnorm, time.perf_counter() - t0))
+            m = m.detach()
+            break
+        loss.backward()
+        g = m.grad.detach()
+        m = m.detach()
+        torch.cuda.synchronize()
+        hist.append((it, rnorm, time.perf_counter() - t0))
+        if callback:
+            callback(it, m, rnorm)
+        gg = _dot_r(g, g)
+        p = -g if p is None else -g + (gg / gg_prev) * p
+        gg_prev = gg
+        with torch.no_grad():
+            q = op.demigrate(p)
+            alpha = -_dot_r(g, p) / _dot_r(q, q)
+            m = m + alpha * p
+    return m, hist
+
+
+def cgls(op, d_obs, niter, refl0=None):
+    """The same least-squares problem by CGLS without autograd: one demigration and one migration
+    per iteration, residual updated by recursion.  Returns (m, history) like lsm_cg."""
+    import torch
+    m = op.zeros_image() if refl0 is None else refl0.detach().clone()
+    r = d_obs - op.demigrate(m) if refl0 is not None else d_obs.clone()
+    s = op.migrate(r)
+    p = s.clone()
+    gamma = _dot_r(s, s)
+    hist = []
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    hist.append((0, float(np.sqrt(_dot_r(r, r))), 0.0))
+    for it in range(niter):
+        q = op.demigrate(p)
+        alpha = gamma / _dot_r(q, q)
+        m = m + alpha * p
+        r = r - alpha * q
+        s = op.migrate(r)
+        gamma_new = _dot_r(s, s)
+        p = s + (gamma_new / gamma) * p
+        gamma = gamma_new
+        torch.cuda.synchronize()
+        hist.append((it + 1, float(np.sqrt(_dot_r(r, r))), time.perf_counter() - t0))
+    return m, hist

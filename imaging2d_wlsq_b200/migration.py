@@ -108,6 +108,19 @@ class Plan:
         check(lib().img2d_plan_execute(self._h, ptr(wave), ptr(shot), ptr(image), ptr(image_shots),
                                        self._stream(stream)))
 
+    def demigrate(self, refl, wave, data, slab_depth=0, stream=None):
+        """Demigration, the adjoint of execute() with respect to the receiver spectra: writes
+        data = F* refl for the source spectra `wave` (read only).  refl is a float32 (>= nextrap, nx)
+        image; data has the packed wavefield layout and must not alias wave.  Source wavefields are
+        recomputed per slab of `slab_depth` depth steps (0: the library default)."""
+        check(lib().img2d_plan_demigrate(self._h, ptr(refl), ptr(wave), ptr(data), int(slab_depth),
+                                         self._stream(stream)))
+
+    def describe_demigration(self):
+        buf = ctypes.create_string_buffer(512)
+        check(lib().img2d_plan_describe_demigration(self._h, buf, 512))
+        return json.loads(buf.value.decode())
+
     def execute_naive(self, wave, shot, image, stream=None):
         check(lib().img2d_plan_execute_naive(self._h, ptr(wave), ptr(shot), ptr(image), self._stream(stream)))
 

@@ -48,6 +48,7 @@ class Workload:
     shot: np.ndarray = field(default=None)   # packed receiver spectra, complex64
     nextrap: int = 0
     seed: int = 0
+    reflectivity: np.ndarray = field(default=None)  # (nz, nx) float32 (least-squares migration only)
 
     @property
     def ns(self):
@@ -191,9 +192,41 @@ def precision(seed=4, scale=1.0, tables=True, ns=64, nextrap=None, nf=None, nx=N
     return _finish(w, 2.0, 60.0, 25.0, rng, tables)
 
 
+def sparse_reflectivity(nz, nx, density, rng):
+    """Seeded sparse spikes (`density` of the samples, amplitudes N(0, 1)) convolved with the
+    3-sample smoothing kernel [1, 2, 1]/4 along z and along x."""
+    r = np.zeros((nz, nx), dtype=np.float64)
+    n = max(1, int(round(density * nz * nx)))
+    flat = rng.choice(nz * nx, size=n, replace=False)
+    r.reshape(-1)[flat] = rng.standard_normal(n)
+    k = np.array([0.25, 0.5, 0.25])
+    r = ndimage.convolve1d(r, k, axis=0, mode="constant")
+    r = ndimage.convolve1d(r, k, axis=1, mode="constant")
+    return r.astype(np.float32)
+
+
+def lsm(seed=5, scale=1.0, tables=True, ns=64, nz=None, nx=None, nf=None):
+    """Least-squares migration configuration: plain_medium's smooth background and operators,
+    64 full-aperture shots, and a sparse reflectivity (0.5% spikes) from which the observed data
+    are synthesised by demigration on the device."""
+    nz = nz or max(8, int(500 * scale))
+    nx = nx or max(32, int(1024 * scale))
+    rng = np.random.default_rng(seed)
+    v = gaussian_random_field(nz, nx, 50.0 * max(scale, 0.1), 1500.0, 4500.0, rng)
+    ns = max(1, int(ns * min(1.0, scale * 4))) if scale < 1.0 else ns
+    pos = np.linspace(nx / (2 * ns), nx - nx / (2 * ns), ns).astype(np.int32)
+    x0, wdt, pos = _full_aperture(ns, nx, pos)
+    w = Workload("lsm", nz, nx, 10.0, 10.0, nf or max(4, int(256 * scale)), 15,
+                 max(64, int(2000 * scale)), 0.0, None, v, None, x0, wdt, pos, nextrap=nz, seed=seed)
+    w = _finish(w, 2.0, 40.0, 20.0, rng, tables)
+    w.reflectivity = sparse_reflectivity(nz, nx, 0.005, rng)
+    return w
+
+
 WORKLOADS = {
     "plain_small": plain_small,
     "plain_medium": plain_medium,
     "batched_uneven": batched_uneven,
     "precision": precision,
+    "lsm": lsm,
 }

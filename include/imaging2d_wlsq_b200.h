@@ -151,6 +151,25 @@ int img2d_migrate_compact_noalloc(int ns, int nextrap, int nz, int nx, int nf, i
                                   const img2d_c64 *d_tab_forw, const int *shot_x0, const int *shot_nx,
                                   img2d_c64 *d_wave, img2d_c64 *d_shot, float *d_image, void *stream);
 
+/* ------------------------------------------------------------------------------------------
+ * Demigration: the adjoint of img2d_plan_execute's stacked image with respect to the receiver
+ * spectra.  No counterpart in the reference, which only migrates (cpp_src/extrapolation_cpu.cpp:
+ * 11-107 is the forward map F that this is the adjoint of).
+ *
+ * For a fixed source (d_wave, packed like img2d_plan_execute's wave buffer, read only) the
+ * migration is the real-linear map F: receiver spectra d -> image I[l][x], l < nextrap.  This
+ * computes d_data = F* m for the reflectivity m = d_refl (rows [0, nextrap) of an nx-wide float
+ * image), with <F d, m> = Re sum d conj(F* m).  It sweeps the depth steps in reverse order with
+ * the transposed operators and recomputes the source wavefield per slab of slab_depth steps from
+ * checkpoints (slab_depth <= 0: 8).  Writes rows [0, nf) of every shot block of d_data (packed like
+ * d_wave, must not alias it).  Single-table mode only (T_back = conj(T_forw)); uses the FP32 table.
+ * Asynchronous on `stream`; img2d_plan_kernel_ms then times this kernel.
+ * ---------------------------------------------------------------------------------------- */
+int img2d_plan_demigrate(img2d_plan *plan, const float *d_refl, const img2d_c64 *d_wave,
+                         img2d_c64 *d_data, int slab_depth, void *stream);
+/* Kernel configuration of the last demigration on this plan (JSON). */
+int img2d_plan_describe_demigration(const img2d_plan *plan, char *buf, int buflen);
+
 /* Naive comparison form: one kernel launch per (shot, frequency, depth), operators from the
  * compact table, wavefields in global memory.  Same arguments and results as
  * img2d_plan_execute (device pointers).  Used only to measure the batched kernel against. */

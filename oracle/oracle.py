@@ -44,6 +44,9 @@ def _load_oracle():
         o.oracle_migrate_compact_f64.argtypes = [c_int] * 8 + [c_double, _f64, _f64, _c64, c_void_p,
                                                                c_void_p, c_void_p, c_void_p, _c128, _c128,
                                                                c_void_p, c_void_p]
+        o.oracle_demigrate_compact_f64.restype = None
+        o.oracle_demigrate_compact_f64.argtypes = [c_int] * 7 + [c_double, _f64, _f64, _c64, c_void_p, c_void_p,
+                                                                 c_void_p, _c128, _f64, _c128]
         o.oracle_gather_dense_slab.restype = None
         o.oracle_gather_dense_slab.argtypes = [c_int] * 8 + [c_double, _f64, _f64, _c64, c_int, _c64]
         o.oracle_index_table.restype = None
@@ -121,6 +124,37 @@ def migrate_workload_f64(wl, nextrap=None, tab_back=None):
     return migrate_compact_f64(wl.ns, n, wl.nz, wl.nx, wl.nf, wl.nt, wl.M, wl.nk, wl.dk, wl.omega, wl.velocity,
                                wl.table, wl.wave, wl.shot, tab_back=tab_back, shot_x0=wl.shot_x0,
                                shot_nx=wl.shot_nx, offsets=wl.offsets())
+
+
+def demigrate_compact_f64(ns, nextrap, nx, nf, nt, M, nk, dk, omega, velocity, tab_forw, wave, refl,
+                          shot_x0=None, shot_nx=None, offsets=None):
+    """FP64 demigration (adjoint of migrate_compact_f64 with respect to the receiver spectra,
+    single-table mode).  refl: (>= nextrap, nx) reflectivity.  Returns the packed data array
+    (complex128, same layout as wave; rows >= nf of each shot block are zero)."""
+    o = _load_oracle()
+    w = np.ascontiguousarray(wave, dtype=np.complex128)
+    data = np.zeros_like(w)
+    r = np.ascontiguousarray(np.asarray(refl, dtype=np.float64)[:nextrap])
+    x0 = None if shot_x0 is None else np.ascontiguousarray(shot_x0, dtype=np.int32)
+    wn = None if shot_nx is None else np.ascontiguousarray(shot_nx, dtype=np.int32)
+    off = None if offsets is None else np.ascontiguousarray(offsets, dtype=np.int64)
+
+    def p(a):
+        return None if a is None else a.ctypes.data
+
+    o.oracle_demigrate_compact_f64(ns, nextrap, nx, nf, nt, M, nk, float(dk),
+                                   np.ascontiguousarray(omega, dtype=np.float64),
+                                   np.ascontiguousarray(velocity, dtype=np.float64),
+                                   np.ascontiguousarray(tab_forw, dtype=np.complex64), p(x0), p(wn), p(off),
+                                   w, r, data)
+    return data
+
+
+def demigrate_workload_f64(wl, refl, nextrap=None):
+    n = nextrap or wl.nextrap
+    return demigrate_compact_f64(wl.ns, n, wl.nx, wl.nf, wl.nt, wl.M, wl.nk, wl.dk, wl.omega, wl.velocity,
+                                 wl.table, wl.wave, refl, shot_x0=wl.shot_x0, shot_nx=wl.shot_nx,
+                                 offsets=wl.offsets())
 
 
 def gather_dense_slab(l0, nl, nx, x0, w, nf, M, nk, dk, omega, velocity, tab, conj_rows=False):

@@ -333,3 +333,89 @@ void oracle_index_table(int nextrap, int nx, int nf, int nk, double dk, const do
                 out[((long)j * nextrap + l) * nx + i] =
                     oracle_nearest_kappa(omega[j] / vel[(long)l * nx + i], dk, nk);
 }
+
+/* ------------------------------------------------------------------------------------
+ * Demigration (the adjoint of oracle_migrate_compact_f64 with respect to the receiver
+ * spectra, single-table mode: receiver rows conj(tabF)).  No reference counterpart: the
+ * reference only migrates.  For the real inner products <I, m> = sum I*m and
+ * <u, v> = Re sum u*conj(v) this returns data = F* m such that
+ *     <F d, m> = Re sum d * conj(F* m)
+ * for the migration F of extrapolation_cpu.cpp:39-89 (source S fixed, receiver d):
+ *     V_{n-1} = m_{n-1} S_n;   U_l = A_l^T V_l;   V_{l-1} = U_l + m_{l-1} S_l;   F* m = U_0,
+ * where (A_l^T V)[i] = sum_k T(l, i')[k] V[i'], i' = i + M - k, inside the shot window (the
+ * transpose of the zero-halo gather).  The source wavefield of every depth is kept in memory
+ * (small test cases only).  refl: (nextrap, nx) float64; data: packed like wave, rows [0, nf)
+ * of every shot block written.  Float64 throughout.
+ * ----------------------------------------------------------------------------------*/
+void oracle_demigrate_compact_f64(int ns, int nextrap, int nx, int nf, int nt, int M, int nk, double dk,
+                                  const double *omega, const double *vel, const cf32 *tabF,
+                                  const int *x0, const int *wnx, const long *woff,
+                                  const cf64 *wave, const double *refl, cf64 *data)
+{
+    const int L = 2 * M + 1;
+    const long npair = (long)ns * nf;
+    int *idx = (int *)malloc((size_t)nf * nextrap * nx * sizeof(int));
+    for (int j = 0; j < nf; ++j)
+        for (int l = 0; l < nextrap; ++l)
+            for (int i = 0; i < nx; ++i)
+                idx[((long)j * nextrap + l) * nx + i] =
+                    oracle_nearest_kappa(omega[j] / vel[(long)l * nx + i], dk, nk);
+#pragma omp parallel
+    {
+        cf64 *S = (cf64 *)malloc((size_t)(nextrap + 1) * nx * sizeof(cf64));
+        cf64 *V = (cf64 *)malloc((size_t)nx * sizeof(cf64));
+        cf64 *U = (cf64 *)malloc((size_t)nx * sizeof(cf64));
+#pragma omp for schedule(dynamic, 1)
+        for (long p = 0; p < npair; ++p) {
+            int s = (int)(p / nf), j = (int)(p % nf);
+            int xs = x0 ? x0[s] : 0;
+            int w = wnx ? wnx[s] : nx;
+            long base = woff ? woff[s] : (long)s * nt * nx;
+            for (int i = 0; i < w; ++i) S[i] = wave[base + (long)j * w + i];
+            for (int l = 0; l < nextrap; ++l) {
+                const int *ix = idx + ((long)j * nextrap + l) * nx + xs;
+                const cf64 *cur = S + (long)l * w;
+                cf64 *nxt = S + (long)(l + 1) * w;
+                for (int i = 0; i < w; ++i) {
+                    const cf32 *t = tabF + (long)ix[i] * L;
+                    double re = 0, im = 0;
+                    for (int k = 0; k < L; ++k) {
+                        int ii = i + k - M;
+                        if (ii < 0 || ii >= w) continue;
+                        re += (double)t[k].re * cur[ii].re - (double)t[k].im * cur[ii].im;
+                        im += (double)t[k].re * cur[ii].im + (double)t[k].im * cur[ii].re;
+                    }
+                    nxt[i] = (cf64){re, im};
+                }
+            }
+            {
+                const double *m = refl + (long)(nextrap - 1) * nx + xs;
+                const cf64 *Sn = S + (long)nextrap * w;
+                for (int i = 0; i < w; ++i) V[i] = (cf64){m[i] * Sn[i].re, m[i] * Sn[i].im};
+            }
+            for (int l = nextrap - 1; l >= 0; --l) {
+                const int *ix = idx + ((long)j * nextrap + l) * nx + xs;
+                for (int i = 0; i < w; ++i) {
+                    double re = 0, im = 0;
+                    for (int k = 0; k < L; ++k) {
+                        int ii = i + M - k;
+                        if (ii < 0 || ii >= w) continue;
+                        const cf32 *t = tabF + (long)ix[ii] * L + k;
+                        re += (double)t->re * V[ii].re - (double)t->im * V[ii].im;
+                        im += (double)t->re * V[ii].im + (double)t->im * V[ii].re;
+                    }
+                    U[i] = (cf64){re, im};
+                }
+                if (l > 0) {
+                    const double *m = refl + (long)(l - 1) * nx + xs;
+                    const cf64 *Sl = S + (long)l * w;
+                    for (int i = 0; i < w; ++i) V[i] = (cf64){U[i].re + m[i] * Sl[i].re, U[i].im + m[i] * Sl[i].im};
+                } else {
+                    for (int i = 0; i < w; ++i) data[base + (long)j * w + i] = U[i];
+                }
+            }
+        }
+        free(S); free(V); free(U);
+    }
+    free(idx);
+}
