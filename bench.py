@@ -34,6 +34,12 @@ METRIC = "extrapolated pts/s (shot*w*z*x), batched vs plain on 1 GPU; rel-L2 err
 UNIT = "pts/s"
 
 
+# ncu, default migration kernel (variant index 10) on the full batched_uneven launch:
+# dram__bytes_read.sum 98.07 GB + dram__bytes_write.sum 78.56 GB
+DEFAULT_VARIANT_INDEX = 10
+PROFILED_TRAFFIC_BYTES = 176.63e9
+
+
 def parse_args():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
@@ -47,12 +53,15 @@ def parse_args():
     p.add_argument("--no-autotune", action="store_true", help="use the plan's default kernel configuration")
     p.add_argument("--nz", type=int, default=None, help="override depth steps (profiling a reduced case)")
     p.add_argument("--nf", type=int, default=None, help="override frequency count (profiling a reduced case)")
+    p.add_argument("--taps", type=int, default=None,
+                   help="override the operator length 2M+1 (odd; timing the per-step overhead)")
     p.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU-baseline sample time")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-naive", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-lsm", action="store_true", help="skip the demigration / least-squares migration leg")
     p.add_argument("--lsm-iters", type=int, default=10)
+    p.add_argument("--lsm-scale", type=float, default=1.0, help="shrink the lsm configuration (profiling)")
     p.add_argument("--accuracy", action="store_true",
                    help="CPU leg also checks rel-L2 against the FP64 checker on a sub-volume")
     p.add_argument("--kernel", default="auto", choices=["auto", "cluster1", "single"],
@@ -220,13 +229,13 @@ def run_reference_impl(args):
     return 0
 
 
-def lsm_leg(dev, iters):
+def lsm_leg(dev, iters, scale=1.0):
     """Demigration (adjoint) and least-squares migration on the lsm configuration: nz=500, nx=1024,
     nf=256 (2-40 Hz), 31 taps, 64 full-aperture shots, 0.5% sparse reflectivity; observed data
     synthesised by the demigration kernel."""
     import torch
     from imaging2d_wlsq_b200 import lsm, synthetic
-    w = synthetic.lsm()
+    w = synthetic.lsm(scale=scale)
     op = lsm.MigrationOperator.for_workload(w, device=dev)
     m_true = torch.from_numpy(w.reflectivity[:w.nextrap]).to(dev)
     for _ in range(3):
@@ -304,6 +313,10 @@ def main():
     maker = synthetic.WORKLOADS[args.workload]
     over = {k: v for k, v in (("nz", args.nz), ("nf", args.nf)) if v}
     w = maker(seed=100 + rank, scale=args.scale, **over) if world > 1 else maker(scale=args.scale, **over)
+    if args.taps:
+        from imaging2d_wlsq_b200 import operators
+        w.M = (args.taps - 1) // 2
+        w.table = operators.design_compact_table(w.nx, w.dx, w.dz, w.M, w.nk, w.dk)
     om = torch.from_numpy(w.omega).to(dev)
     vel = torch.from_numpy(np.ascontiguousarray(w.velocity)).to(dev)
     tab = torch.from_numpy(w.table).to(dev)
@@ -381,6 +394,14 @@ def main():
                     "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({hbm_src})",
                     "note": "operator rows are served from L2/L1 and reused across the shots of a CTA, "
                             "so this algorithmic-bytes ratio exceeds 1; the FP32 roofline binds"}
+        # DRAM bytes of one launch of the default kernel on the full batched_uneven workload, from one
+        # ncu capture (dram__bytes_read.sum + dram__bytes_write.sum, single pass); other shapes: null
+        if (w.name == "batched_uneven" and args.scale == 1.0 and not (args.nz or args.nf or args.taps)
+                and describe.get("variant") == DEFAULT_VARIANT_INDEX and world == 1):
+            roof["traffic"] = PROFILED_TRAFFIC_BYTES
+            roof["traffic_unit"] = "bytes per launch"
+            roof["traffic_source"] = "profiles/migrate_cluster2_kernel_batched_uneven.md"
+            roof_hbm["traffic_gbs"] = PROFILED_TRAFFIC_BYTES / k_s / 1e9
         extra["roofline"] = roof
         extra["roofline_hbm"] = roof_hbm
         extra["kernel_config"] = describe
@@ -488,7 +509,7 @@ def main():
 
     if rank == 0 and world == 1 and not args.no_lsm:
         try:
-            extra["lsm"] = lsm_leg(dev, args.lsm_iters)
+            extra["lsm"] = lsm_leg(dev, args.lsm_iters, args.lsm_scale)
         except Exception as ex:
             extra["lsm"] = {"error": f"{type(ex).__name__}: {ex}"}
 

@@ -101,6 +101,7 @@ struct Cluster2Variant {
     int nw;
     bool tap_pf, row_pf;
     KernelFn fn;
+    bool stage = false;  // uses the step-ahead shared-memory stage (cluster2_stage_bytes)
 };
 
 static const Cluster2Variant kCluster2[] = {
@@ -111,8 +112,12 @@ static const Cluster2Variant kCluster2[] = {
     {8, true, false, migrate_cluster2_kernel<8, true, false>},
     {8, true, true, migrate_cluster2_kernel<8, true, true>},
     {16, false, false, migrate_cluster2_kernel<16, false, false, true>},  // packed FFMA2 arithmetic
+    {16, false, false, migrate_cluster2_kernel<16, false, false, false, TAB_F32, 1>},  // grouped FMA order
+    {16, false, false, migrate_cluster2_kernel<16, false, false, false, TAB_F32, 2>},  // index prefetch
+    {16, false, false, migrate_cluster2_kernel<16, false, false, false, TAB_F32, 3>},  // both
+    {16, false, false, migrate_cluster2_kernel<16, false, false, false, TAB_F32, 4>, true},  // step-ahead stage
 };
-constexpr int kCluster2Default = 0;
+constexpr int kCluster2Default = 10;  // 16 warps with the step-ahead shared-memory stage
 constexpr int kNumCluster2 = (int)(sizeof(kCluster2) / sizeof(kCluster2[0]));
 
 // Demigration kernels: G lane slots per item, compile-time operator length (0 = runtime length).
@@ -459,13 +464,14 @@ static int build_plan(img2d_plan *p, int ns, int nextrap, int nz, int nx, int nf
     if (tab16) {
         // reduced-precision operator storage: default shape with 16-bit tap loads
         cv = {16, false, false,
-              tab16 == 1 ? migrate_cluster2_kernel<16, false, false, false, TAB_F16>
-                         : migrate_cluster2_kernel<16, false, false, false, TAB_BF16>};
+              tab16 == 1 ? migrate_cluster2_kernel<16, false, false, false, TAB_F16, 4>
+                         : migrate_cluster2_kernel<16, false, false, false, TAB_BF16, 4>,
+              true};
         vsel = kCluster2Default;
     }
     const int pc2 = cv.nw * 32;
-    if (cluster_ok && !(flags & IMG2D_FLAG_CLUSTER_V1) && p->L >= 7 &&
-        cluster2_smem_bytes(M, pc2) + static_reserve <= (size_t)smem_optin) {
+    const size_t smem2 = cluster2_smem_bytes(M, pc2) + (cv.stage ? cluster2_stage_bytes(pc2) : 0);
+    if (cluster_ok && !(flags & IMG2D_FLAG_CLUSTER_V1) && p->L >= 7 && smem2 + static_reserve <= (size_t)smem_optin) {
         const int widest = make_groups(16);
         const int K = (widest + pc2 - 1) / pc2;
         if (K <= 8) {
@@ -473,7 +479,7 @@ static int build_plan(img2d_plan *p, int ns, int nextrap, int nz, int nx, int nf
             p->G = 16;
             p->fixed = true;
             p->fn = cv.fn;
-            p->smem = cluster2_smem_bytes(M, pc2);
+            p->smem = smem2;
             p->max_w = widest;
             p->block = pc2;
             p->variant = vsel;

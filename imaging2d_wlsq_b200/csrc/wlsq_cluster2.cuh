@@ -52,6 +52,21 @@ __host__ __device__ inline size_t cluster2_smem_bytes(int M, int pc)
         c2_[3] = __ffma2_rn(t1_, make_float2(vb.z, vb.w), c2_[3]); c2_[3] = __ffma2_rn(t2_, swb1, c2_[3]); \
     } while (0)
 
+// The same sixteen FMAs grouped by tap component: each accumulator's two FMAs are eight
+// instructions apart and fr / fi stay in one operand slot for eight consecutive FMAs.  Per
+// accumulator the operations and their order are those of IMG2D_MAC8 (bit-identical results).
+#define IMG2D_MAC8G(c, fr, fi, va, vb)                                                  \
+    do {                                                                                \
+        c[0] = fmaf(fr, va.x, c[0]); c[1] = fmaf(fr, va.y, c[1]);                       \
+        c[2] = fmaf(fr, va.z, c[2]); c[3] = fmaf(fr, va.w, c[3]);                       \
+        c[4] = fmaf(fr, vb.x, c[4]); c[5] = fmaf(fr, vb.y, c[5]);                       \
+        c[6] = fmaf(fr, vb.z, c[6]); c[7] = fmaf(fr, vb.w, c[7]);                       \
+        c[0] = fmaf(-fi, va.y, c[0]); c[1] = fmaf(fi, va.x, c[1]);                      \
+        c[2] = fmaf(-fi, va.w, c[2]); c[3] = fmaf(fi, va.z, c[3]);                      \
+        c[4] = fmaf(-fi, vb.y, c[4]); c[5] = fmaf(fi, vb.x, c[5]);                      \
+        c[6] = fmaf(-fi, vb.w, c[6]); c[7] = fmaf(fi, vb.z, c[7]);                      \
+    } while (0)
+
 #define IMG2D_MAC8(c, fr, fi, va, vb)                                                   \
     do {                                                                                \
         c[0] = fmaf(fr, va.x, c[0]); c[0] = fmaf(-fi, va.y, c[0]);                      \
@@ -85,20 +100,42 @@ __device__ __forceinline__ float4 load_tap_pair(const void *row, int i)
     return make_float4(a.x, a.y, b.x, b.y);
 }
 
+// Asynchronous 4-byte global -> shared copies (cp.async), one commit group per depth step.
+__device__ __forceinline__ void cp_async4(void *smem_dst, const void *gsrc)
+{
+    const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+// Shared memory of the step-ahead stage (OPT bit 2): per parity, one 32-bit index word and the
+// Kahan partial and compensation values of every position of the CTA.
+__host__ __device__ inline size_t cluster2_stage_bytes(int pc) { return (size_t)pc * (2 * 4 + 2 * 2 * 4); }
+
 // NWARPS: warps per CTA (positions per CTA = 32 * NWARPS).  TAP_PF: operator tap pairs are loaded one
 // step ahead into a second register set.  ROW_PF: the next depth step's operator rows are prefetched
-// into L1 during the current step.
-template <int NWARPS, bool TAP_PF, bool ROW_PF, bool PACKED = false, int TT = TAB_F32>
+// into L1 during the current step.  OPT bit 0: FMAs grouped by tap component (IMG2D_MAC8G);
+// bit 1: the next depth step's operator indices are prefetched into L1 one step ahead; bit 2: the
+// next step's operator indices and Kahan partial-image rows are copied into shared memory
+// (cp.async) one step ahead, so neither the index loads at the start of a step nor the imaging
+// read-modify-write at its end waits on DRAM.
+template <int NWARPS, bool TAP_PF, bool ROW_PF, bool PACKED = false, int TT = TAB_F32, int OPT = 0>
 __global__ void __launch_bounds__(NWARPS * 32, 1) migrate_cluster2_kernel(MigrateArgs a)
 {
     using S = Cluster2Shape<NWARPS>;
     constexpr int Q = S::Q, G = S::G, P = S::P, X = S::X, PC = S::PC;
+    constexpr bool STAGE = (OPT & 4) != 0;
+    static_assert(!STAGE || Q == X, "the stage gives lane q of a group position q of its block");
     const int M = a.M, L = 2 * a.M + 1;
     const int MP = cluster2_mp(M);
     const int NEXT = PC + 2 * MP;
     extern __shared__ float4 smem[];
     float4 *ext = smem;                     // [NEXT][G]; local position x at index x + MP
     float4 *stg = smem + (size_t)NEXT * G;  // [parity][side][MP][G]; side 0 = left halo, 1 = right
+    // step-ahead stage (STAGE): sidx[parity][PC] index words, spart[parity][partial|comp][PC]
+    unsigned *sidx = reinterpret_cast<unsigned *>(stg + (size_t)4 * MP * G);
+    float *spart = reinterpret_cast<float *>(sidx + 2 * PC);
     __shared__ int s_item;
 
     const unsigned crank = cluster_rank(), csize = cluster_size();
@@ -166,27 +203,65 @@ __global__ void __launch_bounds__(NWARPS * 32, 1) migrate_cluster2_kernel(Migrat
         const uint16_t *idx_j = a.idx + (long long)j * a.idx_jstride;
         const int xg = u0 + c0 + b * X;  // model position of the block's first output
         const bool img_lane = part && q == 0 && blk_active;
-        if (img_lane) {
+        if (img_lane && !STAGE) {
             asm volatile("prefetch.global.L1 [%0];" ::"l"(part + xg));
             asm volatile("prefetch.global.L1 [%0];" ::"l"(cmp + xg));
         }
+        // STAGE: lane q copies, for depth step ls, the aligned index word holding position xg+q and
+        // that position's partial and compensation values; one commit group per step
+        const int spos = b * X + q;
+        const int xq = min(xg + q, a.nx - 1);
+        const bool stage_img = part && c0 + spos < W;
+        auto stage_step = [&](int ls) {
+            if (ls < a.nextrap) {
+                const uint16_t *ip = idx_j + (long long)ls * a.idx_lstride + xq;
+                cp_async4(sidx + (ls & 1) * PC + spos, reinterpret_cast<const void *>(
+                                                              reinterpret_cast<uintptr_t>(ip) & ~(uintptr_t)3));
+                if (stage_img) {
+                    cp_async4(spart + ((ls & 1) * 2 + 0) * PC + spos, part + (long long)ls * a.nx + xg + q);
+                    cp_async4(spart + ((ls & 1) * 2 + 1) * PC + spos, cmp + (long long)ls * a.nx + xg + q);
+                }
+            }
+            cp_async_commit();
+        };
+        if (STAGE) stage_step(0);
 
         for (int l = 0; l < a.nextrap; ++l) {
             const int par = l & 1;
             const uint16_t *idx_l = idx_j + (long long)l * a.idx_lstride;
             int roff[X];  // byte offset of each output's operator row
+            if (STAGE) {
+                // this step's words arrived during the previous step; the group's lanes wrote them
+                cp_async_wait_all();
+                __syncwarp(gmask);
 #pragma unroll
-            for (int jj = 0; jj < X; ++jj) roff[jj] = (int)idx_l[min(xg + jj, a.nx - 1)] * row_bytes;
+                for (int jj = 0; jj < X; ++jj) {
+                    const unsigned wv = sidx[par * PC + b * X + jj];
+                    const int xj = min(xg + jj, a.nx - 1);
+                    roff[jj] = (int)((wv >> (16 * (xj & 1))) & 0xffffu) * row_bytes;
+                }
+                stage_step(l + 1);
+            } else {
+#pragma unroll
+                for (int jj = 0; jj < X; ++jj) roff[jj] = (int)idx_l[min(xg + jj, a.nx - 1)] * row_bytes;
+            }
             if (ROW_PF && l + 1 < a.nextrap) {
                 // lane q of the group fetches the 16-byte pairs of output q's next-step row into L1
                 const uint16_t *idx_n = idx_l + a.idx_lstride;
                 const char *rn = tabb + (long long)idx_n[min(xg + q, a.nx - 1)] * row_bytes;
                 for (int c = 0; c < row_bytes; c += 128) asm volatile("prefetch.global.L1 [%0];" ::"l"(rn + c));
             }
-            if (img_lane && l + 1 < a.nextrap) {
+            if ((OPT & 2) && q == 0 && l + 1 < a.nextrap)
+                asm volatile("prefetch.global.L1 [%0];" ::"l"(idx_l + a.idx_lstride + min(xg, a.nx - 1)));
+            if (img_lane && !STAGE && l + 1 < a.nextrap) {
                 asm volatile("prefetch.global.L1 [%0];" ::"l"(part + (long long)(l + 1) * a.nx + xg));
                 asm volatile("prefetch.global.L1 [%0];" ::"l"(cmp + (long long)(l + 1) * a.nx + xg));
             }
+#define IMG2D_MAC(c, fr, fi, va, vb)                 \
+    do {                                             \
+        if (OPT & 1) IMG2D_MAC8G(c, fr, fi, va, vb); \
+        else IMG2D_MAC8(c, fr, fi, va, vb);          \
+    } while (0)
             float acc[X][8];
 #pragma unroll
             for (int jj = 0; jj < X; ++jj)
@@ -207,7 +282,7 @@ __global__ void __launch_bounds__(NWARPS * 32, 1) migrate_cluster2_kernel(Migrat
                         if ((k & 1) == 0) tp[jj] = load_tap_pair<TT>(tabb + roff[jj], (k >> 1));
                         const float fr = (k & 1) ? tp[jj].z : tp[jj].x;
                         const float fi = (k & 1) ? tp[jj].w : tp[jj].y;
-                        IMG2D_MAC8(acc[jj], fr, fi, va, vb);
+                        IMG2D_MAC(acc[jj], fr, fi, va, vb);
                     }
                 }
             }
@@ -229,7 +304,7 @@ __global__ void __launch_bounds__(NWARPS * 32, 1) migrate_cluster2_kernel(Migrat
                             const float fr = (jj & 1) ? tp[jj].x : tp[jj].z;
                             const float fi = (jj & 1) ? tp[jj].y : tp[jj].w;
                             if (PACKED) IMG2D_MAC8P(acc[jj], fr, fi, va, vb, swa0, swa1, swb0, swb1);
-                            else IMG2D_MAC8(acc[jj], fr, fi, va, vb);
+                            else IMG2D_MAC(acc[jj], fr, fi, va, vb);
                         }
                     }
                     {
@@ -243,7 +318,7 @@ __global__ void __launch_bounds__(NWARPS * 32, 1) migrate_cluster2_kernel(Migrat
                             const float fr = (jj & 1) ? tp[jj].z : tp[jj].x;
                             const float fi = (jj & 1) ? tp[jj].w : tp[jj].y;
                             if (PACKED) IMG2D_MAC8P(acc[jj], fr, fi, va, vb, swa0, swa1, swb0, swb1);
-                            else IMG2D_MAC8(acc[jj], fr, fi, va, vb);
+                            else IMG2D_MAC(acc[jj], fr, fi, va, vb);
                         }
                     }
                 }
@@ -271,7 +346,7 @@ __global__ void __launch_bounds__(NWARPS * 32, 1) migrate_cluster2_kernel(Migrat
                             }
                             const float fr = (jj & 1) ? tp[jj].x : tp[jj].z;
                             const float fi = (jj & 1) ? tp[jj].y : tp[jj].w;
-                            IMG2D_MAC8(acc[jj], fr, fi, va, vb);
+                            IMG2D_MAC(acc[jj], fr, fi, va, vb);
                         }
                     }
                     {
@@ -285,7 +360,7 @@ __global__ void __launch_bounds__(NWARPS * 32, 1) migrate_cluster2_kernel(Migrat
                             }
                             const float fr = (jj & 1) ? tp[jj].z : tp[jj].x;
                             const float fi = (jj & 1) ? tp[jj].w : tp[jj].y;
-                            IMG2D_MAC8(acc[jj], fr, fi, va, vb);
+                            IMG2D_MAC(acc[jj], fr, fi, va, vb);
                         }
                     }
                 }
@@ -304,7 +379,7 @@ __global__ void __launch_bounds__(NWARPS * 32, 1) migrate_cluster2_kernel(Migrat
                         if (even) tp[jj] = load_tap_pair<TT>(tabb + roff[jj], ((L + e - jj) >> 1));
                         const float fr = even ? tp[jj].x : tp[jj].z;
                         const float fi = even ? tp[jj].y : tp[jj].w;
-                        IMG2D_MAC8(acc[jj], fr, fi, va, vb);
+                        IMG2D_MAC(acc[jj], fr, fi, va, vb);
                     }
                 }
             }
@@ -362,7 +437,20 @@ __global__ void __launch_bounds__(NWARPS * 32, 1) migrate_cluster2_kernel(Migrat
                 float img = ia + ib;
 #pragma unroll
                 for (int off = 1; off < Q; off <<= 1) img += __shfl_xor_sync(gmask, img, off);
-                if (prow && q == 0 && c0 + b * X + jj < W) kahan_add(prow + xg + jj, crow + xg + jj, img);
+                if (prow && q == 0 && c0 + b * X + jj < W) {
+                    if (STAGE) {
+                        // kahan_add on the staged values; the stores need not be waited for
+                        float sum = spart[(par * 2 + 0) * PC + b * X + jj];
+                        float c = spart[(par * 2 + 1) * PC + b * X + jj];
+                        const float y = img - c;
+                        const float t = sum + y;
+                        c = (t - sum) - y;
+                        prow[xg + jj] = t;
+                        crow[xg + jj] = c;
+                    } else {
+                        kahan_add(prow + xg + jj, crow + xg + jj, img);
+                    }
+                }
             }
             cluster_wait();
             const float4 *hs = stg + (size_t)((par ^ 1) * 2) * MP * G;
@@ -392,7 +480,9 @@ __global__ void __launch_bounds__(NWARPS * 32, 1) migrate_cluster2_kernel(Migrat
     cluster_wait();
 }
 
+#undef IMG2D_MAC
 #undef IMG2D_MAC8
+#undef IMG2D_MAC8G
 #undef IMG2D_MAC8P
 
 }  // namespace img2d

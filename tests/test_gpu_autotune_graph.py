@@ -22,7 +22,8 @@ def test_autotune_picks_a_configuration_that_matches_the_oracle():
     w = synthetic.batched_uneven(nx=1200, nz=10, nf=6, ns=40)
     om, vel, tab, wave, shot = _dev(w)
     plan, report = migration.tuned_plan(w, om, vel, tab, wave, shot, trial_depths=4, repeats=1)
-    assert len(report) >= 3 and report[0][0] <= report[-1][0]
+    # the chosen configuration is the fastest, or the default within the tie margin of it
+    assert len(report) >= 3 and report[0][0] <= 1.02 * min(r[0] for r in report) + 1e-9
     names = [r[1] for r in report]
     assert "single-cta" in names and any(n.startswith("cluster2") for n in names)
     plan.set_model(om, vel, w.dk, tab)
