@@ -25,6 +25,7 @@ FLAG_GENERIC = 2
 FLAG_NO_CLUSTER = 4
 FLAG_CLUSTER_V1 = 8
 FLAG_VARIANT_SHIFT = 8
+SOURCE_RECOMPUTE, SOURCE_KEEP, SOURCE_REUSE = 0, 1, 2
 FLAG_TABLE_FP16 = 16
 FLAG_TABLE_BF16 = 32
 NOALLOC_SCRATCH_BYTES = 64 << 20
@@ -93,7 +94,7 @@ def load():
     lib.img2d_migrate_compact_noalloc.restype = c_int
     lib.img2d_migrate_compact_noalloc.argtypes = [c_int] * 8 + [c_double] + [c_void_p] * 9
     lib.img2d_plan_demigrate.restype = c_int
-    lib.img2d_plan_demigrate.argtypes = [c_void_p] * 4 + [c_int, c_void_p]
+    lib.img2d_plan_demigrate.argtypes = [c_void_p] * 4 + [c_int, c_int, c_void_p]
     lib.img2d_plan_describe_demigration.restype = c_int
     lib.img2d_plan_describe_demigration.argtypes = [c_void_p, c_char_p, c_int]
     lib.img2d_plan_destroy.restype = None

@@ -51,7 +51,39 @@ struct DemigrateArgs {
     long long work_cta;      // float2 elements per CTA
     int wmax;
     int *counter;
+    // source checkpoints: 0 = per CTA, recomputed in every call; 1 = computed into the per-item
+    // cache ckpt_items[item][nslab][wmax*G]; 2 = read from that cache (no checkpoint pass)
+    int ckpt_mode;
+    float2 *ckpt_items;
 };
+
+// Shared-memory words of one staged operator-index row: the positions [u0-Mp, u0+Wp+Mp) of a window,
+// clipped to [0, nx), copied as aligned 32-bit words of the index table row.
+__host__ __device__ inline int demig_idx_words(int Wp, int Mp) { return (Wp + 2 * Mp) / 2 + 2; }
+
+// Copy the index row of depth step l covering the window into `dst` (cp.async, 4-byte words);
+// returns nothing, the caller commits and waits.  Word k of dst holds table entries 2*(w0+k) and
+// 2*(w0+k)+1 of the row, w0 = max(0, u0-Mp) / 2.
+__device__ __forceinline__ void demig_stage_idx(const DemigrateArgs &a, const uint16_t *idx_j, int l, int u0,
+                                                int Wp, int Mp, unsigned *dst)
+{
+    const int lo = max(0, u0 - Mp) >> 1;
+    const int hi = (min(a.nx, u0 + Wp + Mp) + 1) >> 1;  // words [lo, hi) lie inside the padded row
+    const unsigned *row = reinterpret_cast<const unsigned *>(idx_j + (long long)l * a.idx_lstride);
+    for (int k = lo + (int)threadIdx.x; k < hi; k += blockDim.x) {
+        const unsigned d = (unsigned)__cvta_generic_to_shared(dst + (k - lo));
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(row + k) : "memory");
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+}
+
+// Wavefield slots (positions with pad slots) of one buffer for the widest window.
+__host__ __device__ inline int nslot_max(int wmax, int Mp)
+{
+    const int X = 8;
+    const int Wp = ((wmax + X - 1) / X) * X;
+    return (Mp + Wp + Mp) / X * (X + 1);
+}
 
 // Dense [W][G] layout of one depth plane in the per-CTA work area.
 __device__ __forceinline__ long long plane_elems(const DemigrateArgs &a, int G) { return (long long)a.wmax * G; }
@@ -221,27 +253,53 @@ __global__ void __launch_bounds__(NW * 32, 1) demigrate_kernel(DemigrateArgs a)
         const int Wp = ((W + X - 1) / X) * X;
         const int nslot = (Mp + Wp + Mp) / X * (X + 1);
         float2 *bufA = smem2, *bufB = smem2 + nslot * G;
+        // staged operator-index rows (double buffer) after the two wavefield buffers
+        const int iwords = demig_idx_words(((a.wmax + X - 1) / X) * X, Mp);
+        unsigned *sidx0 = reinterpret_cast<unsigned *>(smem2 + 2 * (long long)nslot_max(a.wmax, Mp) * G);
+        unsigned *sidx1 = sidx0 + iwords;
+        const int ibase = 2 * (max(0, u0 - Mp) >> 1);  // table position of staged entry 0
+        const uint16_t *idx_j = a.idx + (long long)j * a.idx_jstride;
+        if (a.ckpt_mode != 0) ckpt = a.ckpt_items + (long long)it * a.nslab * pe;
+        const int D = a.slab;
+        const int first_l = a.ckpt_mode == 2 ? (a.nslab - 1) * D : 0;
+        demig_stage_idx(a, idx_j, first_l, u0, Wp, Mp, sidx0);
         for (int i = threadIdx.x; i < 2 * nslot * G; i += blockDim.x) smem2[i] = make_float2(0.f, 0.f);
         __syncthreads();
-        // source spectra of the group at frequency j
-        for (int k = grp.seg_begin; k < grp.seg_begin + grp.nseg; ++k) {
-            const int4 sg = a.segs[k];
-            const cpx *ws = a.wave + a.shot_off[sg.x] + (long long)j * sg.w;
-            for (int i = threadIdx.x; i < sg.w; i += blockDim.x) {
-                const cpx S = ws[i];
-                bufA[pad_slot(sg.z - u0 + i + Mp, X) * G + sg.y] = make_float2(S.re, S.im);
+        if (a.ckpt_mode != 2) {
+            // source spectra of the group at frequency j
+            for (int k = grp.seg_begin; k < grp.seg_begin + grp.nseg; ++k) {
+                const int4 sg = a.segs[k];
+                const cpx *ws = a.wave + a.shot_off[sg.x] + (long long)j * sg.w;
+                for (int i = threadIdx.x; i < sg.w; i += blockDim.x) {
+                    const cpx S = ws[i];
+                    bufA[pad_slot(sg.z - u0 + i + Mp, X) * G + sg.y] = make_float2(S.re, S.im);
+                }
             }
         }
+        asm volatile("cp.async.wait_group 0;" ::: "memory");
         __syncthreads();
 
         const int16_t *own_base =
             q < grp.nslots ? a.owner + grp.owner_off + (long long)q * grp.owner_stride : nullptr;
         const int nblocks = Wp / X;
-        const uint16_t *idx_j = a.idx + (long long)j * a.idx_jstride;
+        // cur: staged index row of the current step; the next step's row is copied into nxt while
+        // the current step computes, waited for before the step's closing barrier
+        unsigned *cur = sidx0, *nxt = sidx1;
+        auto step_idx = [&]() { return reinterpret_cast<const uint16_t *>(cur) - ibase; };
+        auto stage_next = [&](int nl) {
+            if (nl >= 0) demig_stage_idx(a, idx_j, nl, u0, Wp, Mp, nxt);
+        };
+        auto end_step = [&]() {
+            asm volatile("cp.async.wait_group 0;" ::: "memory");
+            __syncthreads();
+            unsigned *t = cur; cur = nxt; nxt = t;
+        };
 
-        // One forward step of the source, l -> l+1; optionally keeps S_{l+1} in a dense plane.
-        auto forward_step = [&](int l, float2 *keep) {
-            const uint16_t *idx_l = idx_j + (long long)l * a.idx_lstride;
+        // One forward step of the source, l -> l+1; optionally keeps S_{l+1} in a dense plane;
+        // nl: depth step that comes next (its index row is staged meanwhile), -1 for none.
+        auto forward_step = [&](int l, float2 *keep, int nl) {
+            stage_next(nl);
+            const uint16_t *idx_l = step_idx();
             for (int b = gid; b < nblocks; b += ngroups) {
                 const int xb = Mp + b * X;
                 float re[X], im[X];
@@ -258,28 +316,30 @@ __global__ void __launch_bounds__(NW * 32, 1) demigrate_kernel(DemigrateArgs a)
                     if (keep && xr < W) keep[(long long)xr * G + q] = v;
                 }
             }
-            __syncthreads();
+            end_step();
             float2 *t = bufA; bufA = bufB; bufB = t;
         };
 
-        // Phase 1: checkpoints S_{cD}, c = 0 .. nslab-1.
-        const int D = a.slab;
-        for (int c = 0; c < a.nslab; ++c) {
-            smem_to_plane<G, X>(bufA, ckpt + (long long)c * pe, W, Mp);
-            if (c == a.nslab - 1) break;
-            for (int l = c * D; l < (c + 1) * D; ++l) forward_step(l, nullptr);
+        // Phase 1: checkpoints S_{cD}, c = 0 .. nslab-1 (skipped when they come from the cache).
+        if (a.ckpt_mode != 2) {
+            for (int c = 0; c < a.nslab; ++c) {
+                smem_to_plane<G, X>(bufA, ckpt + (long long)c * pe, W, Mp);
+                if (c == a.nslab - 1) break;
+                for (int l = c * D; l < (c + 1) * D; ++l) forward_step(l, nullptr, l + 1);
+            }
+            __syncthreads();
         }
-        __syncthreads();
 
         // Phase 2: slabs in reverse depth order.
         for (int c = a.nslab - 1; c >= 0; --c) {
             const int lb = c * D;
             const int le = lb + D < a.nextrap ? lb + D : a.nextrap;
-            if (c != a.nslab - 1) {
+            if (c != a.nslab - 1 || a.ckpt_mode == 2) {
                 plane_to_smem<G, X>(bufA, ckpt + (long long)c * pe, W, Mp);
                 __syncthreads();
             }
-            for (int l = lb; l < le; ++l) forward_step(l, slabbuf + (long long)(l - lb) * pe);
+            // the last forward step is followed by the backward step at the same depth
+            for (int l = lb; l < le; ++l) forward_step(l, slabbuf + (long long)(l - lb) * pe, l + 1 < le ? l + 1 : l);
             // V_{le-1}: m_{le-1} S_{le} on the deepest slab, else the state saved by the slab below
             {
                 const float *mrow = a.refl + (long long)(le - 1) * a.nx + u0;
@@ -299,7 +359,9 @@ __global__ void __launch_bounds__(NW * 32, 1) demigrate_kernel(DemigrateArgs a)
             }
             __syncthreads();
             for (int l = le - 1; l >= lb; --l) {
-                const uint16_t *idx_l = idx_j + (long long)l * a.idx_lstride;
+                // next: the step above, or the next slab's first forward step
+                stage_next(l > lb ? l - 1 : (c > 0 ? (c - 1) * D : -1));
+                const uint16_t *idx_l = step_idx();
                 // where U_l goes and which source term joins it
                 const bool to_save = (l == lb) && (l > 0);
                 const float2 *Sl = (l > lb) ? slabbuf + (long long)(l - 1 - lb) * pe
@@ -333,7 +395,7 @@ __global__ void __launch_bounds__(NW * 32, 1) demigrate_kernel(DemigrateArgs a)
                         }
                     }
                 }
-                __syncthreads();
+                end_step();
                 if (!to_save) {
                     float2 *t = bufA; bufA = bufB; bufB = t;
                 }

@@ -148,7 +148,8 @@ static size_t demig_smem_bytes(int G, int W, int M)
     const int X = 8;
     const int Mp = ((M + X - 1) / X) * X;
     const int Wp = ((W + X - 1) / X) * X;
-    return 2 * (size_t)((Mp + Wp + Mp) / X * (X + 1)) * G * sizeof(float2);
+    return 2 * (size_t)((Mp + Wp + Mp) / X * (X + 1)) * G * sizeof(float2) +
+           2 * (size_t)demig_idx_words(Wp, Mp) * sizeof(unsigned);
 }
 
 static const ClusterKernel *find_cluster(int L)
@@ -311,6 +312,8 @@ struct img2d_plan {
     size_t adj_smem = 0;
     void (*adj_fn)(img2d::DemigrateArgs) = nullptr;
     img2d::DevBuf adj_items, adj_groups, adj_segs, adj_owner, adj_work, adj_counter;
+    img2d::DevBuf adj_cache;   // source checkpoints kept per item (IMG2D_SOURCE_KEEP)
+    bool adj_cache_valid = false;
 };
 
 namespace img2d {
@@ -684,6 +687,7 @@ static int launch(img2d_plan *p, MigrateArgs a, float *d_image, float *d_image_s
 static int set_model(img2d_plan *p, const double *d_omega, const double *d_vel, double dk,
                      const cpx *d_tabF, const cpx *d_tabB, cudaStream_t st)
 {
+    p->adj_cache_valid = false;
     if (!d_omega || !d_vel || !d_tabF || !(dk > 0.0))
         return fail(IMG2D_EINVAL, "set_model needs omega, velocity, tab_forw and dk > 0");
     if (p->mode == OP_TWO && !d_tabB) return fail(IMG2D_EINVAL, "two-table mode needs tab_back");
@@ -716,6 +720,7 @@ static int demig_prepare(img2d_plan *p, int slab)
     slab = std::min(slab, p->nextrap);
     const int nslab = (p->nextrap + slab - 1) / slab;
     if (p->adj_fn && p->adj_slab == slab) return IMG2D_OK;
+    p->adj_cache_valid = false;  // the checkpoint layout depends on the slab depth
     int dev = 0, smem_optin = 0, nsm = 0;
     IMG2D_CUDA(cudaGetDevice(&dev));
     IMG2D_CUDA(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
@@ -932,14 +937,24 @@ int img2d_plan_execute(img2d_plan *p, img2d_c64 *d_wave, img2d_c64 *d_shot, floa
 }
 
 int img2d_plan_demigrate(img2d_plan *p, const float *d_refl, const img2d_c64 *d_wave, img2d_c64 *d_data,
-                         int slab_depth, void *stream)
+                         int slab_depth, int source_mode, void *stream)
 {
     if (!p) return fail(IMG2D_EINVAL, "plan is NULL");
     if (!d_refl || !d_wave || !d_data) return fail(IMG2D_EINVAL, "null device pointer");
     if ((const void *)d_wave == (const void *)d_data) return fail(IMG2D_EINVAL, "data must not alias wave");
     if (p->mode != OP_CONJ) return fail(IMG2D_EINVAL, "demigration supports the single-table mode only");
+    if (source_mode < IMG2D_SOURCE_RECOMPUTE || source_mode > IMG2D_SOURCE_REUSE)
+        return fail(IMG2D_EINVAL, "source_mode must be IMG2D_SOURCE_RECOMPUTE, _KEEP or _REUSE");
     int rc;
     if ((rc = demig_prepare(p, slab_depth))) return rc;
+    if (source_mode == IMG2D_SOURCE_REUSE && !p->adj_cache_valid)
+        return fail(IMG2D_EINVAL, "no kept source checkpoints on this plan (call with IMG2D_SOURCE_KEEP first, "
+                                  "after the last set_model, with the same slab depth)");
+    const long long cache_elems =
+        (long long)p->adj_items_n * p->adj_nslab * p->adj_wmax * p->adj_G;  // float2 per kept item
+    if (source_mode == IMG2D_SOURCE_KEEP) {
+        if ((rc = p->adj_cache.ensure((size_t)cache_elems * sizeof(float2)))) return rc;
+    }
     cudaStream_t st = (cudaStream_t)stream;
     DemigrateArgs a{};
     a.nextrap = p->nextrap;
@@ -965,6 +980,8 @@ int img2d_plan_demigrate(img2d_plan *p, const float *d_refl, const img2d_c64 *d_
     a.work_cta = (long long)(p->adj_nslab + p->adj_slab + 1) * p->adj_wmax * p->adj_G;
     a.wmax = p->adj_wmax;
     a.counter = p->adj_counter.as<int>();
+    a.ckpt_mode = source_mode;
+    a.ckpt_items = source_mode == IMG2D_SOURCE_RECOMPUTE ? nullptr : p->adj_cache.as<float2>();
     IMG2D_CUDA(cudaMemsetAsync(p->adj_counter.p, 0, sizeof(int), st));
     if (p->timing && !p->ev0) {
         IMG2D_CUDA(cudaEventCreate(&p->ev0));
@@ -977,6 +994,7 @@ int img2d_plan_demigrate(img2d_plan *p, const float *d_refl, const img2d_c64 *d_
         IMG2D_CUDA(cudaEventRecord(p->ev1, st));
         p->ev_recorded = true;
     }
+    if (source_mode == IMG2D_SOURCE_KEEP) p->adj_cache_valid = true;
     return IMG2D_OK;
 }
 
@@ -987,9 +1005,9 @@ int img2d_plan_describe_demigration(const img2d_plan *p, char *buf, int buflen)
     snprintf(buf, buflen,
              "{\"kernel\": \"demigrate\", \"G\": %d, \"X\": 8, \"L\": %d, \"grid\": %d, \"block\": %d, "
              "\"smem\": %zu, \"items\": %d, \"max_union_width\": %d, \"slab\": %d, \"slabs\": %d, "
-             "\"workspace_bytes\": %zu}",
+             "\"workspace_bytes\": %zu, \"source_cache_bytes\": %zu}",
              p->adj_G, p->L, p->adj_grid, p->adj_block, p->adj_smem, p->adj_items_n, p->adj_wmax, p->adj_slab,
-             p->adj_nslab, p->adj_work.bytes);
+             p->adj_nslab, p->adj_work.bytes, p->adj_cache.bytes);
     return IMG2D_OK;
 }
 
@@ -1007,7 +1025,7 @@ size_t img2d_plan_workspace_bytes(const img2d_plan *p)
     return p->items.bytes + p->groups.bytes + p->segs.bytes + p->owner.bytes + p->shot_off.bytes +
            p->idx.bytes + p->tabF.bytes + p->tabB.bytes + p->tab16buf.bytes + p->partial.bytes + p->comp.bytes + p->counter.bytes +
            p->naive_buf.bytes + p->adj_items.bytes + p->adj_groups.bytes + p->adj_segs.bytes + p->adj_owner.bytes +
-           p->adj_work.bytes + p->adj_counter.bytes;
+           p->adj_work.bytes + p->adj_counter.bytes + p->adj_cache.bytes;
 }
 
 int img2d_plan_describe(const img2d_plan *p, char *buf, int buflen)

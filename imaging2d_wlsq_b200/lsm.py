@@ -31,24 +31,28 @@ class MigrationOperator:
     wave    device complex64 source spectra in the plan's packed layout; kept, never modified
     """
 
-    def __init__(self, plan, wave, slab_depth=0):
+    def __init__(self, plan, wave, slab_depth=0, keep_source=True):
+        """keep_source: the first demigration keeps the source checkpoints on the plan and later
+        ones reuse them (the source does not change between calls); False recomputes every time."""
         import torch
         self.plan = plan
         self.wave = wave
         self.slab_depth = slab_depth
+        self.keep_source = keep_source
+        self._kept = False
         self.nextrap, self.nx = plan.nextrap, plan.nx
         self.device = wave.device
         self._src = torch.empty_like(wave)
         self._rec = torch.empty_like(wave)
 
     @classmethod
-    def for_workload(cls, w, device=None, slab_depth=0, **plan_kw):
+    def for_workload(cls, w, device=None, slab_depth=0, keep_source=True, **plan_kw):
         import torch
         dev = device or torch.device("cuda")
         plan = Plan.for_workload(w, **plan_kw)
         plan.set_model(torch.from_numpy(w.omega).to(dev), torch.from_numpy(np.ascontiguousarray(w.velocity)).to(dev),
                        w.dk, torch.from_numpy(w.table).to(dev))
-        return cls(plan, torch.from_numpy(w.wave).to(dev), slab_depth=slab_depth)
+        return cls(plan, torch.from_numpy(w.wave).to(dev), slab_depth=slab_depth, keep_source=keep_source)
 
     def zeros_data(self):
         import torch
@@ -71,8 +75,12 @@ class MigrationOperator:
         """F* m: receiver spectra (packed layout) of the reflectivity `refl` (nextrap, nx)."""
         import torch
         data = self.zeros_data() if data is None else data
-        self.plan.demigrate(refl.contiguous(), self.wave, data, slab_depth=self.slab_depth,
+        source = "recompute"
+        if self.keep_source:
+            source = "reuse" if self._kept else "keep"
+        self.plan.demigrate(refl.contiguous(), self.wave, data, slab_depth=self.slab_depth, source=source,
                             stream=torch.cuda.current_stream(self.device))
+        self._kept = self._kept or source == "keep"
         return data
 
 

@@ -109,12 +109,15 @@ class Plan:
         check(lib().img2d_plan_execute(self._h, ptr(wave), ptr(shot), ptr(image), ptr(image_shots),
                                        self._stream(stream)))
 
-    def demigrate(self, refl, wave, data, slab_depth=0, stream=None):
+    def demigrate(self, refl, wave, data, slab_depth=0, source="recompute", stream=None):
         """Demigration, the adjoint of execute() with respect to the receiver spectra: writes
         data = F* refl for the source spectra `wave` (read only).  refl is a float32 (>= nextrap, nx)
         image; data has the packed wavefield layout and must not alias wave.  Source wavefields are
-        recomputed per slab of `slab_depth` depth steps (0: the library default)."""
-        check(lib().img2d_plan_demigrate(self._h, ptr(refl), ptr(wave), ptr(data), int(slab_depth),
+        recomputed per slab of `slab_depth` depth steps (0: the library default) from checkpoints;
+        source="keep" keeps those checkpoints on the plan and "reuse" reads them instead of
+        computing them (same `wave` as the keeping call, no set_model in between)."""
+        mode = {"recompute": _lib.SOURCE_RECOMPUTE, "keep": _lib.SOURCE_KEEP, "reuse": _lib.SOURCE_REUSE}[source]
+        check(lib().img2d_plan_demigrate(self._h, ptr(refl), ptr(wave), ptr(data), int(slab_depth), mode,
                                          self._stream(stream)))
 
     def describe_demigration(self):

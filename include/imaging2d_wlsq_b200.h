@@ -164,9 +164,22 @@ int img2d_migrate_compact_noalloc(int ns, int nextrap, int nz, int nx, int nf, i
  * checkpoints (slab_depth <= 0: 8).  Writes rows [0, nf) of every shot block of d_data (packed like
  * d_wave, must not alias it).  Single-table mode only (T_back = conj(T_forw)); uses the FP32 table.
  * Asynchronous on `stream`; img2d_plan_kernel_ms then times this kernel.
+ *
+ * source_mode: the source wavefield does not depend on the reflectivity, so repeated
+ * demigrations with the same source (a least-squares migration loop) can keep its checkpoints.
+ *   IMG2D_SOURCE_RECOMPUTE  checkpoints in per-CTA scratch, recomputed by this call, not kept;
+ *   IMG2D_SOURCE_KEEP       checkpoints computed by this call and kept on the plan
+ *                           (items x slabs x window x slots x 8 bytes of device memory);
+ *   IMG2D_SOURCE_REUSE      the kept checkpoints are read instead of computed (the checkpoint pass,
+ *                           a third of the work, is skipped).  The caller guarantees the same
+ *                           d_wave contents as the keeping call; img2d_plan_set_model and a
+ *                           different slab_depth discard the kept checkpoints (IMG2D_EINVAL).
  * ---------------------------------------------------------------------------------------- */
+#define IMG2D_SOURCE_RECOMPUTE 0
+#define IMG2D_SOURCE_KEEP 1
+#define IMG2D_SOURCE_REUSE 2
 int img2d_plan_demigrate(img2d_plan *plan, const float *d_refl, const img2d_c64 *d_wave,
-                         img2d_c64 *d_data, int slab_depth, void *stream);
+                         img2d_c64 *d_data, int slab_depth, int source_mode, void *stream);
 /* Kernel configuration of the last demigration on this plan (JSON). */
 int img2d_plan_describe_demigration(const img2d_plan *plan, char *buf, int buflen);
 

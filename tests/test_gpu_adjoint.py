@@ -152,3 +152,35 @@ def test_least_squares_migration_reduces_residual_and_solvers_agree():
     assert np.allclose(r_ag, r_cg, rtol=1e-3)
     assert rel_l2(m_ag.cpu().numpy(), m_cg.cpu().numpy()) <= 1e-3
     op.plan.close()
+
+
+@pytest.mark.parametrize("case", ["uneven_L35", "runtime_L11", "full_L31"])
+@pytest.mark.parametrize("slab", [0, 3])
+def test_source_checkpoint_modes_agree(case, slab):
+    """Recomputed, kept and reused source checkpoints give bit-identical demigrated data (the
+    checkpoints are the same arithmetic), and match the FP64 oracle."""
+    import torch
+    from imaging2d_wlsq_b200._lib import LibraryError
+    w = CASES[case]()
+    op = _op(w, slab)
+    plan = op.plan
+    m = torch.from_numpy(np.random.default_rng(4).standard_normal((w.nextrap, w.nx)).astype(np.float32)).cuda()
+    outs = {}
+    with pytest.raises(LibraryError, match="kept source checkpoints"):
+        plan.demigrate(m, op.wave, op.zeros_data(), slab_depth=slab, source="reuse")
+    for mode in ("recompute", "keep", "reuse", "reuse"):
+        d = op.zeros_data()
+        plan.demigrate(m, op.wave, d, slab_depth=slab, source=mode)
+        outs.setdefault(mode, []).append(d.cpu().numpy())
+    ref = outs["recompute"][0]
+    for mode, arrs in outs.items():
+        for arr in arrs:
+            assert np.array_equal(arr, ref), mode
+    assert rel_l2(ref, oracle.demigrate_workload_f64(w, m.cpu().numpy().astype(np.float64))) <= 1e-5
+    assert plan.describe_demigration()["source_cache_bytes"] > 0
+    # a new model discards the kept checkpoints
+    plan.set_model(torch.from_numpy(w.omega).cuda(), torch.from_numpy(np.ascontiguousarray(w.velocity)).cuda(),
+                   w.dk, torch.from_numpy(w.table).cuda())
+    with pytest.raises(LibraryError, match="kept source checkpoints"):
+        plan.demigrate(m, op.wave, op.zeros_data(), slab_depth=slab, source="reuse")
+    plan.close()
