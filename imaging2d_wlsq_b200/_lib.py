@@ -91,6 +91,8 @@ def load():
     lib.img2d_plan_kernel_ms.argtypes = [c_void_p, POINTER(ctypes.c_float)]
     lib.img2d_measure_fp32_peak.restype = c_int
     lib.img2d_measure_fp32_peak.argtypes = [POINTER(c_double)]
+    lib.img2d_measure_l2_bandwidth.restype = c_int
+    lib.img2d_measure_l2_bandwidth.argtypes = [POINTER(c_double)]
     lib.img2d_migrate_compact_noalloc.restype = c_int
     lib.img2d_migrate_compact_noalloc.argtypes = [c_int] * 8 + [c_double] + [c_void_p] * 9
     lib.img2d_plan_demigrate.restype = c_int

@@ -205,6 +205,33 @@ __global__ void naive_unpack_kernel(const float4 *__restrict__ buf, int w, int M
     shot[i] = cpx{v.z, -v.w};
 }
 
+// L2 read probe: every thread streams float4 from an L2-resident buffer with ld.global.cg (L2 only,
+// no L1 allocation); four independent accumulators keep many loads in flight.
+__global__ void l2_read_probe_kernel(const float4 *__restrict__ buf, long long n4, int iters, float *out)
+{
+    float4 acc[4] = {};
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    const long long t0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    for (int it = 0; it < iters; ++it) {
+        long long i = t0;
+        for (; i + 3 * stride < n4; i += 4 * stride) {
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const float4 v = __ldcg(buf + i + u * stride);
+                acc[u].x += v.x; acc[u].y += v.y; acc[u].z += v.z; acc[u].w += v.w;
+            }
+        }
+        for (; i < n4; i += stride) {
+            const float4 v = __ldcg(buf + i);
+            acc[0].x += v.x; acc[0].y += v.y; acc[0].z += v.z; acc[0].w += v.w;
+        }
+    }
+    float s = 0.f;
+#pragma unroll
+    for (int u = 0; u < 4; ++u) s += acc[u].x + acc[u].y + acc[u].z + acc[u].w;
+    out[t0] = s;
+}
+
 // FP32 FMA probe: 16 independent chains per thread so the FMA pipe, not latency, limits it.
 __global__ void fma_probe_kernel(float *out, int iters)
 {
@@ -1088,6 +1115,49 @@ int img2d_measure_fp32_peak(double *tflops)
     cudaEventDestroy(e1);
     // 16 chains x 8 FMAs per iteration per thread, 2 flops per FMA
     *tflops = 2.0 * 128.0 * iters * (double)blocks * threads / (best * 1e-3) * 1e-12;
+    return IMG2D_OK;
+}
+
+int img2d_measure_l2_bandwidth(double *gbs)
+{
+    if (!gbs) return fail(IMG2D_EINVAL, "gbs is NULL");
+    int rc;
+    if ((rc = check_device())) return rc;
+    int dev = 0, nsm = 0;
+    IMG2D_CUDA(cudaGetDevice(&dev));
+    IMG2D_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    Scratch sc;
+    const long long bytes = 32ll << 20;  // resident in L2 (126 MB on B200)
+    const long long n4 = bytes / 16;
+    const int blocks = nsm * 4, threads = 512, iters = 64;
+    float4 *buf;
+    float *out;
+    if ((rc = sc.alloc(&buf, (size_t)bytes))) return rc;
+    if ((rc = sc.alloc(&out, (size_t)blocks * threads * sizeof(float)))) return rc;
+    IMG2D_CUDA(cudaMemset(buf, 0, (size_t)bytes));
+    l2_read_probe_kernel<<<blocks, threads>>>(buf, n4, 2, out);  // warm the lines into L2
+    IMG2D_CUDA(cudaGetLastError());
+    cudaEvent_t e0, e1;
+    IMG2D_CUDA(cudaEventCreate(&e0));
+    IMG2D_CUDA(cudaEventCreate(&e1));
+    float best = 1e30f;
+    for (int r = 0; r < 3; ++r) {
+        cudaEventRecord(e0);
+        l2_read_probe_kernel<<<blocks, threads>>>(buf, n4, iters, out);
+        cudaEventRecord(e1);
+        cudaError_t e = cudaEventSynchronize(e1);
+        if (e != cudaSuccess) {
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+            return fail(IMG2D_ECUDA, std::string("l2 probe: ") + cudaGetErrorString(e));
+        }
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        best = std::min(best, ms);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    *gbs = (double)bytes * iters / (best * 1e-3) * 1e-9;
     return IMG2D_OK;
 }
 

@@ -16,6 +16,11 @@ with <F d, m> = Re sum d conj(F* m).  Least-squares migration solves min_m 1/2 |
 
 Data live on the device in the packed wavefield layout of the plan (complex64, per shot nt rows of
 that shot's aperture); images are float32 (nextrap, nx).
+
+Several GPUs: each rank builds its operator on its own shots (sharding.assign_shots) and passes the
+process group.  Its migration all-reduces the image, so images (reflectivity, gradient, search
+direction) are the same on every rank, and inner products of data (residuals stay with their shots)
+are all-reduced; the solvers below then run unchanged, one image all-reduce per migration.
 """
 import time
 
@@ -31,14 +36,16 @@ class MigrationOperator:
     wave    device complex64 source spectra in the plan's packed layout; kept, never modified
     """
 
-    def __init__(self, plan, wave, slab_depth=0, keep_source=True):
+    def __init__(self, plan, wave, slab_depth=0, keep_source=True, group=None):
         """keep_source: the first demigration keeps the source checkpoints on the plan and later
-        ones reuse them (the source does not change between calls); False recomputes every time."""
+        ones reuse them (the source does not change between calls); False recomputes every time.
+        group: torch.distributed process group when the shots are shared out over ranks."""
         import torch
         self.plan = plan
         self.wave = wave
         self.slab_depth = slab_depth
         self.keep_source = keep_source
+        self.group = group
         self._kept = False
         self.nextrap, self.nx = plan.nextrap, plan.nx
         self.device = wave.device
@@ -46,13 +53,22 @@ class MigrationOperator:
         self._rec = torch.empty_like(wave)
 
     @classmethod
-    def for_workload(cls, w, device=None, slab_depth=0, keep_source=True, **plan_kw):
+    def for_workload(cls, w, device=None, slab_depth=0, keep_source=True, group=None, **plan_kw):
         import torch
         dev = device or torch.device("cuda")
         plan = Plan.for_workload(w, **plan_kw)
         plan.set_model(torch.from_numpy(w.omega).to(dev), torch.from_numpy(np.ascontiguousarray(w.velocity)).to(dev),
                        w.dk, torch.from_numpy(w.table).to(dev))
-        return cls(plan, torch.from_numpy(w.wave).to(dev), slab_depth=slab_depth, keep_source=keep_source)
+        return cls(plan, torch.from_numpy(w.wave).to(dev), slab_depth=slab_depth, keep_source=keep_source,
+                   group=group)
+
+    def data_dot(self, a, b):
+        """Real inner product of two data vectors, summed over the ranks that share the shots."""
+        return _allreduce_scalar(_dot_r(a, b), self.group, self.device)
+
+    def image_dot(self, a, b):
+        """Real inner product of two images (replicated on every rank: no communication)."""
+        return _dot_r(a, b)
 
     def zeros_data(self):
         import torch
@@ -69,6 +85,9 @@ class MigrationOperator:
         self._src.copy_(self.wave)
         self._rec.copy_(data)
         self.plan.execute(self._src, self._rec, image, stream=torch.cuda.current_stream(self.device))
+        if self.group is not None:
+            import torch.distributed as dist
+            dist.all_reduce(image, group=self.group)
         return image
 
     def demigrate(self, refl, data=None):
@@ -144,6 +163,22 @@ def _dot_r(a, b):
     return float(torch.sum(a.double() * b.double()))
 
 
+def _allreduce_scalar(v, group, device):
+    if group is None:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device=device)
+    dist.all_reduce(t, group=group)
+    return float(t.item())
+
+
+def _sync(op):
+    import torch
+    if op.device.type == "cuda":
+        torch.cuda.synchronize(op.device)
+
+
 def dot_product_test(op, seed=0, data=None, refl=None):
     """<F d, m> against Re sum d conj(F* m) for seeded Gaussian d and m.  Returns
     (lhs, rhs, rel, rel_norms) with rel = |lhs - rhs| / max(|lhs|, |rhs|) and
@@ -157,16 +192,16 @@ def dot_product_test(op, seed=0, data=None, refl=None):
     if refl is None:
         refl = torch.randn((op.nextrap, op.nx), dtype=torch.float32, device=op.device, generator=g)
     img = op.migrate(data)
-    lhs = _dot_r(img, refl)
-    rhs = _dot_r(data, op.demigrate(refl))
-    scale = np.sqrt(_dot_r(img, img) * _dot_r(refl, refl))
+    lhs = op.image_dot(img, refl)
+    rhs = op.data_dot(data, op.demigrate(refl))
+    scale = np.sqrt(op.image_dot(img, img) * op.image_dot(refl, refl))
     return lhs, rhs, abs(lhs - rhs) / max(abs(lhs), abs(rhs)), abs(lhs - rhs) / scale
 
 
 def misfit(op, refl, d_obs):
     """J(m) = 1/2 ||F* m - d_obs||^2 in float64."""
     r = op.demigrate(refl) - d_obs
-    return 0.5 * _dot_r(r, r)
+    return 0.5 * op.data_dot(r, r)
 
 
 def finite_difference_check(op, refl, d_obs, points, h):
@@ -176,6 +211,7 @@ def finite_difference_check(op, refl, d_obs, points, h):
     import torch
     m = refl.detach().clone().requires_grad_(True)
     r = demigrate(m, op) - d_obs
+    # each rank back-propagates its shots' misfit; the migration in the backward sums the ranks
     loss = 0.5 * (r.real.double().pow(2).sum() + r.imag.double().pow(2).sum())
     loss.backward()
     grad = m.grad.detach()
@@ -202,32 +238,32 @@ def lsm_cg(op, d_obs, niter, refl0=None, callback=None):
     p = None
     gg_prev = None
     hist = []
-    torch.cuda.synchronize()
+    _sync(op)
     t0 = time.perf_counter()
     for it in range(niter + 1):
         m.requires_grad_(True)
         r = demigrate(m, op) - d_obs
         rr = r.real.double().pow(2).sum() + r.imag.double().pow(2).sum()
         loss = 0.5 * rr
-        rnorm = float(rr.detach().sqrt())
+        rnorm = float(np.sqrt(_allreduce_scalar(float(rr.detach()), op.group, op.device)))
         if it == niter:
-            torch.cuda.synchronize()
+            _sync(op)
             hist.append((it, rnorm, time.perf_counter() - t0))
             m = m.detach()
             break
         loss.backward()
         g = m.grad.detach()
         m = m.detach()
-        torch.cuda.synchronize()
+        _sync(op)
         hist.append((it, rnorm, time.perf_counter() - t0))
         if callback:
             callback(it, m, rnorm)
-        gg = _dot_r(g, g)
+        gg = op.image_dot(g, g)
         p = -g if p is None else -g + (gg / gg_prev) * p
         gg_prev = gg
         with torch.no_grad():
             q = op.demigrate(p)
-            alpha = -_dot_r(g, p) / _dot_r(q, q)
+            alpha = -op.image_dot(g, p) / op.data_dot(q, q)
             m = m + alpha * p
     return m, hist
 
@@ -240,20 +276,20 @@ def cgls(op, d_obs, niter, refl0=None):
     r = d_obs - op.demigrate(m) if refl0 is not None else d_obs.clone()
     s = op.migrate(r)
     p = s.clone()
-    gamma = _dot_r(s, s)
+    gamma = op.image_dot(s, s)
     hist = []
-    torch.cuda.synchronize()
+    _sync(op)
     t0 = time.perf_counter()
-    hist.append((0, float(np.sqrt(_dot_r(r, r))), 0.0))
+    hist.append((0, float(np.sqrt(op.data_dot(r, r))), 0.0))
     for it in range(niter):
         q = op.demigrate(p)
-        alpha = gamma / _dot_r(q, q)
+        alpha = gamma / op.data_dot(q, q)
         m = m + alpha * p
         r = r - alpha * q
         s = op.migrate(r)
-        gamma_new = _dot_r(s, s)
+        gamma_new = op.image_dot(s, s)
         p = s + (gamma_new / gamma) * p
         gamma = gamma_new
-        torch.cuda.synchronize()
-        hist.append((it + 1, float(np.sqrt(_dot_r(r, r))), time.perf_counter() - t0))
+        _sync(op)
+        hist.append((it + 1, float(np.sqrt(op.data_dot(r, r))), time.perf_counter() - t0))
     return m, hist

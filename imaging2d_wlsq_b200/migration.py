@@ -59,6 +59,13 @@ def fp32_peak_tflops():
     return v.value
 
 
+def l2_read_bandwidth_gbs():
+    """Measured L2 read bandwidth of the current GPU (GB/s)."""
+    v = ctypes.c_double()
+    check(lib().img2d_measure_l2_bandwidth(ctypes.byref(v)))
+    return v.value
+
+
 class Plan:
     """Device-resident migration plan (torch CUDA tensors in, torch CUDA tensors out)."""
 

@@ -124,6 +124,10 @@ int img2d_plan_kernel_ms(img2d_plan *plan, float *ms);
  * FMA chains (the denominator of the FP32 roofline; not part of the migration path). */
 int img2d_measure_fp32_peak(double *tflops);
 
+/* L2 read bandwidth of the current device in GB/s: all SMs stream a 32 MB L2-resident buffer with
+ * L2-only loads (the denominator of the L2 roofline of the operator gathers). */
+int img2d_measure_l2_bandwidth(double *gbs);
+
 /* ------------------------------------------------------------------------------------------
  * No-allocation entry point.  No counterpart in the reference: the reference libraries allocate
  * their device memory inside every call.
