@@ -62,6 +62,7 @@ def parse_args():
     p.add_argument("--no-lsm", action="store_true", help="skip the demigration / least-squares migration leg")
     p.add_argument("--lsm-iters", type=int, default=10)
     p.add_argument("--lsm-scale", type=float, default=1.0, help="shrink the lsm configuration (profiling)")
+    p.add_argument("--no-frontend", action="store_true", help="skip the front-end (wavelet, record spectra) leg")
     p.add_argument("--accuracy", action="store_true",
                    help="CPU leg also checks rel-L2 against the FP64 checker on a sub-volume")
     p.add_argument("--kernel", default="auto", choices=["auto", "cluster1", "single"],
@@ -293,6 +294,70 @@ def lsm_leg(dev, iters, scale=1.0):
     }
     op.plan.close()
     return out
+
+
+def frontend_leg(dev, w):
+    """Front end on the workload's shot geometry: time-domain records (ns, nt = 2 nf, nx) float32,
+    resident on the device, to the first nf frequency rows of each shot's aperture; and the source
+    wavelets of all shots (built and transformed).  CPU: the reference's own call of main.py:119
+    (scipy.fftpack.fft along time) on one shot record, and the wavelet restatement on one shot."""
+    import time as _time
+    import torch
+    import scipy.fftpack as spfft
+    from imaging2d_wlsq_b200 import frontend
+    ns, nx, nf = w.ns, w.nx, w.nf
+    nt, dt = 2 * nf, 0.004
+    g = torch.Generator(device=dev).manual_seed(11)
+    rec = torch.randn((ns, nt, nx), generator=g, device=dev, dtype=torch.float32)
+    out = torch.empty(int(nf * w.shot_nx.astype(np.int64).sum()), dtype=torch.complex64, device=dev)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+
+    def timed(fn, reps=3):
+        fn()
+        best = 1e30
+        for _ in range(reps):
+            e0.record()
+            fn()
+            e1.record()
+            e1.synchronize()
+            best = min(best, e0.elapsed_time(e1) / 1e3)
+        return best
+
+    t_rec = timed(lambda: frontend.records_to_spectra(rec, nf, shot_x0=w.shot_x0, shot_nx=w.shot_nx, out=out))
+    del rec
+    sx = w.shot_pos.astype(np.float64) * w.dx
+    src_out = torch.empty(ns * nf * nx, dtype=torch.complex64, device=dev)
+
+    def sources():
+        st = frontend.ricker_sources(ns, nt, nx, dt, 0.0, w.dx, 10.0, 2000.0, sx, device=dev)
+        frontend.records_to_spectra(st, nf, out=src_out)
+
+    t_src = timed(sources)
+    samples = int(nt * w.shot_nx.astype(np.int64).sum())
+    # CPU: one shot, the reference's transform call and the wavelet restatement
+    one = np.random.default_rng(11).standard_normal((nt, nx)).astype(np.float32)
+    c0 = _time.perf_counter()
+    spfft.fft(one, axis=0)[:nf]
+    c_fft = _time.perf_counter() - c0
+    from oracle import frontend_oracle
+    c0 = _time.perf_counter()
+    frontend_oracle.ricker_sources(1, nt, nx, dt, 0.0, w.dx, 10.0, 2000.0, sx[:1])
+    c_ric = _time.perf_counter() - c0
+    return {
+        "workload": f"ns={ns} nt={nt} nx={nx} nf={nf}, receiver records on the {w.name} apertures "
+                    f"(mean {w.shot_nx.mean():.0f} traces); sources full aperture",
+        "records": {"value": samples / t_rec, "unit": "time samples/s", "ms": t_rec * 1e3,
+                    "hbm_gbs": (4.0 * ns * nt * nx + 8.0 * 2 * ns * (nt // 2 + 1) * nx + 8.0 * nf * w.shot_nx.sum())
+                               / t_rec / 1e9,
+                    "kernel": "cuFFT real-to-complex along time + pack_spectra_kernel (first nf rows, apertures)"},
+        "sources": {"value": ns * nt * nx / t_src, "unit": "time samples/s", "ms": t_src * 1e3},
+        "cpu_reference_fft": {"value": nt * nx / c_fft, "unit": "time samples/s", "ms_per_shot": c_fft * 1e3,
+                              "cores": 1, "kind": "reference",
+                              "sample": f"scipy.fftpack.fft of one ({nt}, {nx}) record, the call of main.py:119"},
+        "cpu_port_ricker": {"value": nt * nx / c_ric, "unit": "time samples/s", "ms_per_shot": c_ric * 1e3,
+                            "cores": 1, "kind": "port", "sample": "oracle wavelet restatement, one shot"},
+    }
 
 
 def workload_config(w, args):
@@ -527,6 +592,12 @@ def main():
                                  "sub_volume": f"first {sub_n} depth steps, all shots and frequencies",
                                  "reference": "FP64 CPU checker"}
             plan_a.close()
+
+    if rank == 0 and world == 1 and not args.no_frontend:
+        try:
+            extra["frontend"] = frontend_leg(dev, w)
+        except Exception as ex:
+            extra["frontend"] = {"error": f"{type(ex).__name__}: {ex}"}
 
     if rank == 0 and world == 1 and not args.no_lsm:
         try:

@@ -91,6 +91,10 @@ def load():
     lib.img2d_plan_kernel_ms.argtypes = [c_void_p, POINTER(ctypes.c_float)]
     lib.img2d_measure_fp32_peak.restype = c_int
     lib.img2d_measure_fp32_peak.argtypes = [POINTER(c_double)]
+    lib.img2d_ricker_sources.restype = c_int
+    lib.img2d_ricker_sources.argtypes = [c_int] * 3 + [c_double] * 6 + [c_void_p] * 3
+    lib.img2d_records_to_spectra.restype = c_int
+    lib.img2d_records_to_spectra.argtypes = [c_int] * 5 + [c_void_p] * 5
     lib.img2d_measure_l2_bandwidth.restype = c_int
     lib.img2d_measure_l2_bandwidth.argtypes = [POINTER(c_double)]
     lib.img2d_migrate_compact_noalloc.restype = c_int

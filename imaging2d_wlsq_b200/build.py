@@ -41,7 +41,7 @@ def _stale(target, deps):
 def build_cuda(force=False, verbose_ptxas=False):
     if force or _stale(LIB, SOURCES + HEADERS):
         cmd = [NVCC, *ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-shared",
-               "-o", LIB, *SOURCES]
+               "-o", LIB, *SOURCES, "-lcufft"]
         if verbose_ptxas:
             cmd.insert(1, "-Xptxas=-v")
         _run(cmd)

@@ -1,6 +1,7 @@
 // C ABI of the B200 extrapolation + imaging library: plans, kernel dispatch and the
 // reference-compatible entry points.  Declarations and contracts: include/imaging2d_wlsq_b200.h.
 #include <algorithm>
+#include <map>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -9,10 +10,12 @@
 #include <vector>
 
 #include "../../include/imaging2d_wlsq_b200.h"
+#include <cufft.h>
 #include "wlsq_kernels.cuh"
 #include "wlsq_cluster.cuh"
 #include "wlsq_cluster2.cuh"
 #include "wlsq_adjoint.cuh"
+#include "wlsq_frontend.cuh"
 
 namespace img2d {
 
@@ -1115,6 +1118,101 @@ int img2d_measure_fp32_peak(double *tflops)
     cudaEventDestroy(e1);
     // 16 chains x 8 FMAs per iteration per thread, 2 flops per FMA
     *tflops = 2.0 * 128.0 * iters * (double)blocks * threads / (best * 1e-3) * 1e-12;
+    return IMG2D_OK;
+}
+
+int img2d_ricker_sources(int ns, int nt, int nx, double dt, double x_first, double dx, double depth_offset,
+                         double v, double fpeak, const double *src_x, float *d_out, void *stream)
+{
+    int rc;
+    if ((rc = check_device())) return rc;
+    if (ns <= 0 || nt <= 0 || nx <= 0 || !(dt > 0.0) || !(dx > 0.0) || !(v > 0.0))
+        return fail(IMG2D_EINVAL, "invalid source-wavelet dimensions or spacing");
+    if (!src_x || !d_out) return fail(IMG2D_EINVAL, "null pointer argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    Scratch sc;
+    double *d_sx;
+    if ((rc = sc.alloc(&d_sx, (size_t)ns * sizeof(double)))) return rc;
+    IMG2D_CUDA(cudaMemcpyAsync(d_sx, src_x, (size_t)ns * sizeof(double), cudaMemcpyHostToDevice, st));
+    const long long total = (long long)ns * nt * nx;
+    const int blocks = (int)std::min<long long>((total + 255) / 256, 148 * 32);
+    ricker_sources_kernel<<<blocks, 256, 0, st>>>(ns, nt, nx, dt, x_first, dx, depth_offset, v, fpeak, d_sx, d_out);
+    IMG2D_CUDA(cudaGetLastError());
+    IMG2D_CUDA(cudaStreamSynchronize(st));  // the source positions are freed on return
+    return IMG2D_OK;
+}
+
+int img2d_records_to_spectra(int ns, int nt, int nx, int nf, int nt_rows, const float *d_records,
+                             const int *shot_x0, const int *shot_nx, img2d_c64 *d_out, void *stream)
+{
+    int rc;
+    if ((rc = check_device())) return rc;
+    if (ns <= 0 || nt <= 0 || nx <= 0 || nf <= 0 || nf > nt || nt_rows < nf)
+        return fail(IMG2D_EINVAL, "invalid dimensions (need ns, nt, nx > 0, 0 < nf <= nt, nt_rows >= nf)");
+    if (!d_records || !d_out) return fail(IMG2D_EINVAL, "null pointer argument");
+    std::vector<int> x0(ns, 0), w(ns, nx);
+    std::vector<long long> off(ns, 0);
+    long long acc = 0;
+    for (int s = 0; s < ns; ++s) {
+        if (shot_x0) x0[s] = shot_x0[s];
+        if (shot_nx) w[s] = shot_nx[s];
+        if (x0[s] < 0 || w[s] <= 0 || x0[s] + w[s] > nx)
+            return fail(IMG2D_EINVAL, "shot " + std::to_string(s) + " aperture outside [0, nx)");
+        off[s] = acc;
+        acc += (long long)nt_rows * w[s];
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    // shots per transform group: their spectra (nt/2+1 rows) in at most 512 MB of scratch
+    const long long shot_spec = (long long)(nt / 2 + 1) * nx;
+    const int group = (int)std::max<long long>(1, std::min<long long>(ns, (512ll << 20) / (shot_spec * 8)));
+    int dev = 0;
+    IMG2D_CUDA(cudaGetDevice(&dev));
+    // One plan per (device, nt, nx), kept for the process: the nx transforms of length nt of one
+    // shot, element (t, x) at x + t*nx in and at x + j*nx out; shots are issued one by one.  The
+    // plans are shared, so the lock is held while this call issues its transforms.
+    static std::mutex plan_mu;
+    static std::map<std::vector<long long>, cufftHandle> plans;
+    std::lock_guard<std::mutex> plan_lock(plan_mu);
+    const std::vector<long long> key = {dev, nt, nx};
+    auto itp = plans.find(key);
+    if (itp == plans.end()) {
+        int n[1] = {nt};
+        int inembed[1] = {nt}, onembed[1] = {nt / 2 + 1};
+        cufftHandle h;
+        if (cufftCreate(&h) != CUFFT_SUCCESS) return fail(IMG2D_ECUDA, "cufftCreate failed");
+        size_t ws = 0;
+        if (cufftMakePlanMany(h, 1, n, inembed, nx, 1, onembed, nx, 1, CUFFT_R2C, nx, &ws) != CUFFT_SUCCESS) {
+            cufftDestroy(h);
+            return fail(IMG2D_ECUDA, "cufftMakePlanMany (real-to-complex along time) failed");
+        }
+        itp = plans.emplace(key, h).first;
+    }
+    const cufftHandle plan = itp->second;
+    if (cufftSetStream(plan, st) != CUFFT_SUCCESS) return fail(IMG2D_ECUDA, "cufftSetStream failed");
+    Scratch sc;
+    int *d_x0, *d_w;
+    long long *d_off;
+    cpx *d_spec;
+    if ((rc = sc.alloc(&d_x0, ns * sizeof(int)))) return rc;
+    if ((rc = sc.alloc(&d_w, ns * sizeof(int)))) return rc;
+    if ((rc = sc.alloc(&d_off, ns * sizeof(long long)))) return rc;
+    if ((rc = sc.alloc(&d_spec, (size_t)group * shot_spec * sizeof(cpx)))) return rc;
+    IMG2D_CUDA(cudaMemcpyAsync(d_x0, x0.data(), ns * sizeof(int), cudaMemcpyHostToDevice, st));
+    IMG2D_CUDA(cudaMemcpyAsync(d_w, w.data(), ns * sizeof(int), cudaMemcpyHostToDevice, st));
+    IMG2D_CUDA(cudaMemcpyAsync(d_off, off.data(), ns * sizeof(long long), cudaMemcpyHostToDevice, st));
+    for (int s0 = 0; s0 < ns; s0 += group) {
+        const int nsc = std::min(group, ns - s0);
+        for (int k = 0; k < nsc; ++k) {
+            cufftReal *in = const_cast<cufftReal *>(d_records + (long long)(s0 + k) * nt * nx);
+            cufftComplex *o = reinterpret_cast<cufftComplex *>(d_spec + (long long)k * shot_spec);
+            if (cufftExecR2C(plan, in, o) != CUFFT_SUCCESS) return fail(IMG2D_ECUDA, "cufftExecR2C failed");
+        }
+        const long long total = (long long)nsc * nf * nx;
+        const int blocks = (int)std::min<long long>((total + 255) / 256, 148 * 32);
+        pack_spectra_kernel<<<blocks, 256, 0, st>>>(s0, nsc, nt, nx, nf, d_spec, d_x0, d_w, d_off, (cpx *)d_out);
+        IMG2D_CUDA(cudaGetLastError());
+    }
+    IMG2D_CUDA(cudaStreamSynchronize(st));  // descriptors and spectra scratch are freed on return
     return IMG2D_OK;
 }
 

@@ -129,6 +129,32 @@ int img2d_measure_fp32_peak(double *tflops);
 int img2d_measure_l2_bandwidth(double *gbs);
 
 /* ------------------------------------------------------------------------------------------
+ * Front end: the per-shot data preparation of main.py:111-123 on the device.
+ *
+ * img2d_ricker_sources replaces util.makeRickerWavelet (py_src/operatorsPreparation/util.py:47-58,
+ * wavelet util.py:10-14) for ns single sources: d_out (ns, nt, nx) float32 gets
+ *   (1 - 2 pi^2 f^2 tau^2) exp(-pi^2 f^2 tau^2) / sqrt(r),  r = sqrt(depth_offset^2 + (x_i - src_x[s])^2),
+ *   tau = float32(j dt - r / v),  x_i = x_first + i dx,
+ * with f = fpeak (the reference uses 30 Hz).  main.py:114-122 calls it with x_first = xmin + dx,
+ * src_x[s] = xmin + shot_isx[s] dx, depth_offset = dz - zinit and v = velocity[0][0].  src_x is a
+ * host array; the call returns when d_out is written.
+ *
+ * img2d_records_to_spectra replaces scipy.fftpack.fft(record, axis=0) of main.py:118-123 followed
+ * by the use of its first nf rows: d_records (ns, nt, nx) float32 time-domain traces (receiver
+ * records or the wavelets above) -> d_out packed like the migration's wave/shot buffers (per shot
+ * nt_rows rows of that shot's aperture [shot_x0[s], shot_x0[s] + shot_nx[s]), NULL = full
+ * aperture), rows j < nf set to sum_t rec[t][x] exp(-2 pi i j t / nt), other rows untouched.  The
+ * transform is a single-precision real-to-complex cuFFT along time (as the reference's transform of
+ * float32 records is single precision), rows above nt/2 by conjugate symmetry.  shot_x0 / shot_nx
+ * are host arrays; the call returns when d_out is written.
+ * ---------------------------------------------------------------------------------------- */
+int img2d_ricker_sources(int ns, int nt, int nx, double dt, double x_first, double dx,
+                         double depth_offset, double v, double fpeak, const double *src_x,
+                         float *d_out, void *stream);
+int img2d_records_to_spectra(int ns, int nt, int nx, int nf, int nt_rows, const float *d_records,
+                             const int *shot_x0, const int *shot_nx, img2d_c64 *d_out, void *stream);
+
+/* ------------------------------------------------------------------------------------------
  * No-allocation entry point.  No counterpart in the reference: the reference libraries allocate
  * their device memory inside every call.
  *

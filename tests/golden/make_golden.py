@@ -10,6 +10,11 @@ Writes
                        (py_src/operatorsPreparation/{preparation,util}.py, run with numba) for a
                        small odd-width model: createWLSQoperators, make{Forw,Back}PSoperators,
                        createKappa, find_nearest and makeTableOfOperators.
+  frontend_case.npz    the demo's data-preparation parameters (main.py:105-123), the reference's
+                       util.makeRickerWavelet output and the time-domain CSV record of one shot, and
+                       the first nw rows of scipy.fftpack.fft of that record (the receiver spectra the
+                       demo feeds to the extrapolation); the source spectra of all shots are in
+                       demo_case.npz
   demo_case.npz        the reference demo (demo-data/, problemSetup.txt) reduced to the compact form
                        this library consumes: smoothed velocity, angular frequencies, kappa step,
                        compact forward/backward tables (rows = op[M] @ psOp[k], the numpy call of
@@ -134,7 +139,30 @@ def demo_case():
     print(f"demo: reference CPU library vs shipped final_image.csv rel-L2 {rel:.3e}")
 
 
+def frontend_case():
+    vel0 = np.genfromtxt(os.path.join(REF, "demo-data", "velmod.csv"), delimiter=",")
+    vel = 1.0 / ndimage.gaussian_filter(1.0 / vel0, sigma=2)     # main.py:40-41
+    cfg = parse_setup(os.path.join(REF, "demo-data", "problemSetup.txt"))
+    nz, nx = vel.shape
+    nt, nw = int(cfg["nt"]), int(cfg["nw"])
+    dz = (cfg["zmax"] - cfg["zmin"]) / nz
+    dx = (cfg["xmax"] - cfg["xmin"]) / nx
+    dt = (cfg["tmax"] - cfg["tmin"]) / nt
+    files = glob.glob(os.path.join(REF, "demo-data", "seismicShots") + "/*.csv")
+    isx = [int(re.search(r"seis(.+?)_", os.path.basename(f)).group(1)) for f in files]
+    v = vel[0, 0]
+    tj = [j * dt for j in range(nt)]
+    xi = [cfg["xmin"] + (i + 1) * dx for i in range(nx)]
+    wavelet = util.makeRickerWavelet([cfg["xmin"] + isx[0] * dx], cfg["zinit"], nt, nx, tj, xi, dz, v)
+    rec = np.genfromtxt(files[0], delimiter=",", dtype=np.float32)
+    rec_f = spfft.fft(rec, axis=0)[:nw]
+    np.savez_compressed(os.path.join(HERE, "frontend_case.npz"), nt=nt, nw=nw, nx=nx, dx=dx, dz=dz, dt=dt,
+                        xmin=cfg["xmin"], zinit=cfg["zinit"], v=v, shot_isx=np.array(isx),
+                        wavelet_t=wavelet, rec_t=rec, rec_f=rec_f.astype(np.complex64))
+
+
 if __name__ == "__main__":
     operators_small()
+    frontend_case()
     demo_case()
     print("wrote", os.listdir(HERE))
