@@ -10,6 +10,7 @@ operator choice main.py:66 uses (gIdx = M everywhere, util.py:19-21), a gather o
 (nk, 2M+1) table built here: T[l, j, i, :] = compact[find_nearest(kappa, w[j] / v[l, i])].
 The CUDA library consumes the compact table directly.
 """
+import cmath
 import math
 
 import numpy as np
@@ -84,7 +85,10 @@ def create_wlsq_operators(N, M, kx, x, only_symmetric=False):
     Nk = 2 * N + 1
     kx = np.asarray(kx)
     x = np.asarray(x)
-    full = np.exp(1j * kx[:, None] * x[None, :]).astype(np.complex64)  # (Nk, L)
+    # element by element with cmath.exp as preparation.py:75-90 does: numpy's vectorised complex exp
+    # differs from it in the last bits for some arguments, which survives the cast to complex64
+    full = np.array([[cmath.exp(1j * kx[n] * x[m]) for m in range(L)] for n in range(Nk)],
+                    dtype=np.complex128).astype(np.complex64)  # (Nk, L)
     op = np.zeros((L, L, Nk), dtype=np.complex64)
     gs = [M] if only_symmetric else range(L)
     for g in gs:

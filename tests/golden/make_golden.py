@@ -15,6 +15,10 @@ Writes
                        the first nw rows of scipy.fftpack.fft of that record (the receiver spectra the
                        demo feeds to the extrapolation); the source spectra of all shots are in
                        demo_case.npz
+  driver_case.npz      inputs of the reference driver for two demo shots (the raw velocity model, the
+                       two time-domain CSV records and their source indices) and the image that the
+                       reference flow (main.py: its Python operator design and data preparation, then
+                       oracle/_ref/extrapolation_cpu.so on the dense tables) produces from them
   demo_case.npz        the reference demo (demo-data/, problemSetup.txt) reduced to the compact form
                        this library consumes: smoothed velocity, angular frequencies, kappa step,
                        compact forward/backward tables (rows = op[M] @ psOp[k], the numpy call of
@@ -161,8 +165,51 @@ def frontend_case():
                         wavelet_t=wavelet, rec_t=rec, rec_f=rec_f.astype(np.complex64))
 
 
+def driver_case(nshots=2):
+    vel0 = np.genfromtxt(os.path.join(REF, "demo-data", "velmod.csv"), delimiter=",")
+    vel = 1.0 / ndimage.gaussian_filter(1.0 / vel0, sigma=2)     # main.py:40-41
+    cfg = parse_setup(os.path.join(REF, "demo-data", "problemSetup.txt"))
+    nz, nx = vel.shape
+    nt, nw, M = int(cfg["nt"]), int(cfg["nw"]), int(cfg["M"])
+    dz = (cfg["zmax"] - cfg["zmin"]) / nz
+    nextrap = math.ceil((cfg["zfinal"] - cfg["zinit"]) / dz)
+    dx = (cfg["xmax"] - cfg["xmin"]) / nx
+    dt = (cfg["tmax"] - cfg["tmin"]) / nt
+    N = int((nx - 1) / 2)
+    kx = np.fft.fftfreq(nx) * nx * (2 * math.pi / float(cfg["xmax"] - cfg["xmin"]))
+    dw = 2 * math.pi / float(cfg["tmax"] - cfg["tmin"])
+    w = np.fft.fftfreq(nt) * nt * dw
+    wmax = +(0.5 * nt - 1) * dw
+    xil = np.array([(-M * dx) + i * dx for i in range(2 * M + 1)], dtype=np.float32)
+    op = prep.createWLSQoperators(N, M, kx, xil)
+    kappa = util.createKappa(np.amax(vel), np.amin(vel), dw, wmax, 0.25)
+    gidx = util.defWLSQIndices(nx=nx, M=M, flip=False, sym=True, extent=5)
+    tf = prep.makeTableOfOperators(nextrap, nx, nw, kappa, kx, w, vel, gidx, op,
+                                   prep.makeForwPSoperators(kappa, kx, dz))       # main.py:82-88
+    tb = prep.makeTableOfOperators(nextrap, nx, nw, kappa, kx, w, vel, gidx, op,
+                                   prep.makeBackPSoperators(kappa, kx, dz))
+    files = glob.glob(os.path.join(REF, "demo-data", "seismicShots") + "/*.csv")[:nshots]
+    isx = [int(re.search(r"seis(.+?)_", os.path.basename(f)).group(1)) for f in files]
+    v = vel[0, 0]
+    tj = [j * dt for j in range(nt)]
+    xi = [cfg["xmin"] + (i + 1) * dx for i in range(nx)]
+    records = np.stack([np.genfromtxt(f, delimiter=",", dtype=np.float32) for f in files])
+    src = np.zeros((nshots, nt, nx), dtype=np.complex64)
+    rec = np.zeros((nshots, nt, nx), dtype=np.complex64)
+    for s in range(nshots):
+        src[s] = spfft.fft(util.makeRickerWavelet([cfg["xmin"] + isx[s] * dx], cfg["zinit"], nt, nx, tj, xi, dz, v),
+                           axis=0)
+        rec[s] = spfft.fft(records[s], axis=0)
+    image = np.zeros((nshots, nz, nx), dtype=np.float32)
+    oracle.ref_extrapolate(nshots, nextrap, nz, nx, nw, nt, M, np.ascontiguousarray(tf, dtype=np.complex64),
+                           np.ascontiguousarray(tb, dtype=np.complex64), src, rec, image)
+    np.savez_compressed(os.path.join(HERE, "driver_case.npz"), velmod=vel0, records=records, shot_isx=np.array(isx),
+                        image=image.sum(axis=0))
+
+
 if __name__ == "__main__":
     operators_small()
     frontend_case()
+    driver_case()
     demo_case()
     print("wrote", os.listdir(HERE))
