@@ -15,6 +15,7 @@
 #include "wlsq_cluster.cuh"
 #include "wlsq_cluster2.cuh"
 #include "wlsq_adjoint.cuh"
+#include "wlsq_adjoint_cluster.cuh"
 #include "wlsq_frontend.cuh"
 
 namespace img2d {
@@ -133,6 +134,25 @@ struct DemigKernel {
 #define IMG2D_DEMIG(G, L) {G, L, demigrate_kernel<G, L, kAdjWarps>}
 #define IMG2D_DEMIG_G(G) IMG2D_DEMIG(G, 0), IMG2D_DEMIG(G, 25), IMG2D_DEMIG(G, 31), IMG2D_DEMIG(G, 35), IMG2D_DEMIG(G, 55)
 static const DemigKernel kDemig[] = {IMG2D_DEMIG_G(2), IMG2D_DEMIG_G(4), IMG2D_DEMIG_G(8)};
+
+struct DemigClusterKernel {
+    int L;
+    DemigFn fn;
+};
+static const DemigClusterKernel kDemigCluster[] = {
+    {0, demigrate_cluster_kernel<0>},   {25, demigrate_cluster_kernel<25>}, {31, demigrate_cluster_kernel<31>},
+    {35, demigrate_cluster_kernel<35>}, {55, demigrate_cluster_kernel<55>},
+};
+
+static DemigFn find_demig_cluster(int L)
+{
+    DemigFn generic = nullptr;
+    for (const auto &k : kDemigCluster) {
+        if (k.L == L) return k.fn;
+        if (k.L == 0) generic = k.fn;
+    }
+    return generic;
+}
 
 static DemigFn find_demig(int G, int L)
 {
@@ -339,6 +359,8 @@ struct img2d_plan {
     std::vector<int> slot_order, slot_end;
     // demigration (adjoint) launch state, built on its first call
     int adj_G = 0, adj_grid = 0, adj_items_n = 0, adj_wmax = 0, adj_block = 0, adj_slab = 0, adj_nslab = 0;
+    int adj_cluster = 0;               // CTAs per cluster of the cluster demigration kernel, 0 = single CTA
+    long long adj_work_cta = 0, adj_cache_item = 0;  // float2 elements: per-CTA work area, kept per item
     size_t adj_smem = 0;
     void (*adj_fn)(img2d::DemigrateArgs) = nullptr;
     img2d::DevBuf adj_items, adj_groups, adj_segs, adj_owner, adj_work, adj_counter;
@@ -759,30 +781,72 @@ static int demig_prepare(img2d_plan *p, int slab)
     std::vector<GroupDesc> groups;
     std::vector<int4> segs;
     std::vector<int16_t> owner;
-    int G = 8, widest = 0;
-    for (;; G >>= 1) {
-        widest = pack_groups(p, G, groups, segs, owner);
-        if (demig_smem_bytes(G, widest, p->M) + static_reserve <= (size_t)smem_optin) break;
-        if (G == 2) return fail(IMG2D_EINVAL, "aperture too wide for the demigration kernel's shared memory");
+    int G = 8, widest = 0, K = 0;
+    DemigFn fn = nullptr;
+    size_t smem = 0;
+    // Cluster kernel (16 slots per item, 512 positions per CTA) when there are enough slots to fill
+    // it and the widest window fits 8 CTAs; otherwise the single-CTA kernel.
+    if (p->n_slots >= 12 && !(p->flags & IMG2D_FLAG_NO_CLUSTER) &&
+        demigc_smem_bytes(p->M) + static_reserve <= (size_t)smem_optin) {
+        widest = pack_groups(p, 16, groups, segs, owner);
+        const int k = (widest + kDcPC - 1) / kDcPC;
+        if (k <= 8) {
+            K = k;
+            G = 16;
+            fn = find_demig_cluster(p->L);
+            smem = demigc_smem_bytes(p->M);
+        }
     }
-    // fewer slots than lanes: smaller groups leave fewer idle lanes
-    while (G > 2 && (int)p->slot_order.size() <= G / 2) G >>= 1;
-    widest = pack_groups(p, G, groups, segs, owner);
-    DemigFn fn = find_demig(G, p->L);
+    if (!K) {
+        for (;; G >>= 1) {
+            widest = pack_groups(p, G, groups, segs, owner);
+            if (demig_smem_bytes(G, widest, p->M) + static_reserve <= (size_t)smem_optin) break;
+            if (G == 2) return fail(IMG2D_EINVAL, "aperture too wide for the demigration kernel's shared memory");
+        }
+        // fewer slots than lanes: smaller groups leave fewer idle lanes
+        while (G > 2 && (int)p->slot_order.size() <= G / 2) G >>= 1;
+        widest = pack_groups(p, G, groups, segs, owner);
+        fn = find_demig(G, p->L);
+        smem = demig_smem_bytes(G, widest, p->M);
+    }
     if (!fn) return fail(IMG2D_EINVAL, "no demigration kernel for this configuration");
-    const size_t smem = demig_smem_bytes(G, widest, p->M);
     IMG2D_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    int bps = 0;
-    IMG2D_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, fn, kAdjWarps * 32, smem));
-    if (bps <= 0) return fail(IMG2D_ECUDA, "demigration kernel does not fit on an SM");
     std::vector<int2> items;
     std::vector<int> gorder(groups.size());
     std::iota(gorder.begin(), gorder.end(), 0);
     std::stable_sort(gorder.begin(), gorder.end(), [&](int a, int b) { return groups[a].W > groups[b].W; });
     for (int g : gorder)
         for (int j = 0; j < p->nf; ++j) items.push_back(make_int2(g, j));
-    const int grid = (int)std::min<size_t>(items.size(), (size_t)nsm * bps);
-    const long long work_cta = (long long)(nslab + slab + 1) * widest * G;
+    int grid = 0;
+    long long work_cta = 0;   // float2 elements of per-CTA work area
+    long long cache_item = 0; // float2 elements of kept checkpoints per item
+    if (K) {
+        cudaLaunchConfig_t cfg{};
+        cudaLaunchAttribute attr{};
+        attr.id = cudaLaunchAttributeClusterDimension;
+        attr.val.clusterDim.x = K;
+        attr.val.clusterDim.y = 1;
+        attr.val.clusterDim.z = 1;
+        cfg.gridDim = dim3(K * 64, 1, 1);
+        cfg.blockDim = dim3(kDcNW * 32, 1, 1);
+        cfg.dynamicSmemBytes = smem;
+        cfg.attrs = &attr;
+        cfg.numAttrs = 1;
+        int nclusters = 0;
+        IMG2D_CUDA(cudaOccupancyMaxActiveClusters(&nclusters, (void *)fn, &cfg));
+        if (nclusters <= 0) return fail(IMG2D_ECUDA, "no demigration cluster of this size fits on the device");
+        grid = (int)std::min<size_t>(items.size(), (size_t)nclusters) * K;
+        const long long pe4 = (long long)kDcPC * kDcQ;  // float4 per plane
+        work_cta = 2 * (long long)(nslab + slab + 1) * pe4;
+        cache_item = 2 * (long long)K * nslab * pe4;
+    } else {
+        int bps = 0;
+        IMG2D_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, fn, kAdjWarps * 32, smem));
+        if (bps <= 0) return fail(IMG2D_ECUDA, "demigration kernel does not fit on an SM");
+        grid = (int)std::min<size_t>(items.size(), (size_t)nsm * bps);
+        work_cta = (long long)(nslab + slab + 1) * widest * G;
+        cache_item = (long long)nslab * widest * G;
+    }
     int rc;
     if ((rc = p->adj_items.ensure(items.size() * sizeof(int2)))) return rc;
     if ((rc = p->adj_groups.ensure(groups.size() * sizeof(GroupDesc)))) return rc;
@@ -798,7 +862,10 @@ static int demig_prepare(img2d_plan *p, int slab)
     p->adj_grid = grid;
     p->adj_items_n = (int)items.size();
     p->adj_wmax = widest;
-    p->adj_block = kAdjWarps * 32;
+    p->adj_block = K ? kDcNW * 32 : kAdjWarps * 32;
+    p->adj_cluster = K;
+    p->adj_work_cta = work_cta;
+    p->adj_cache_item = cache_item;
     p->adj_slab = slab;
     p->adj_nslab = nslab;
     p->adj_smem = smem;
@@ -980,8 +1047,7 @@ int img2d_plan_demigrate(img2d_plan *p, const float *d_refl, const img2d_c64 *d_
     if (source_mode == IMG2D_SOURCE_REUSE && !p->adj_cache_valid)
         return fail(IMG2D_EINVAL, "no kept source checkpoints on this plan (call with IMG2D_SOURCE_KEEP first, "
                                   "after the last set_model, with the same slab depth)");
-    const long long cache_elems =
-        (long long)p->adj_items_n * p->adj_nslab * p->adj_wmax * p->adj_G;  // float2 per kept item
+    const long long cache_elems = (long long)p->adj_items_n * p->adj_cache_item;  // float2
     if (source_mode == IMG2D_SOURCE_KEEP) {
         if ((rc = p->adj_cache.ensure((size_t)cache_elems * sizeof(float2)))) return rc;
     }
@@ -1007,7 +1073,7 @@ int img2d_plan_demigrate(img2d_plan *p, const float *d_refl, const img2d_c64 *d_
     a.refl = d_refl;
     a.data = (cpx *)d_data;
     a.work = p->adj_work.as<float2>();
-    a.work_cta = (long long)(p->adj_nslab + p->adj_slab + 1) * p->adj_wmax * p->adj_G;
+    a.work_cta = p->adj_work_cta;
     a.wmax = p->adj_wmax;
     a.counter = p->adj_counter.as<int>();
     a.ckpt_mode = source_mode;
@@ -1018,7 +1084,23 @@ int img2d_plan_demigrate(img2d_plan *p, const float *d_refl, const img2d_c64 *d_
         IMG2D_CUDA(cudaEventCreate(&p->ev1));
     }
     if (p->timing) IMG2D_CUDA(cudaEventRecord(p->ev0, st));
-    p->adj_fn<<<p->adj_grid, p->adj_block, p->adj_smem, st>>>(a);
+    if (p->adj_cluster) {
+        cudaLaunchConfig_t cfg{};
+        cudaLaunchAttribute attr{};
+        attr.id = cudaLaunchAttributeClusterDimension;
+        attr.val.clusterDim.x = p->adj_cluster;
+        attr.val.clusterDim.y = 1;
+        attr.val.clusterDim.z = 1;
+        cfg.gridDim = dim3(p->adj_grid, 1, 1);
+        cfg.blockDim = dim3(p->adj_block, 1, 1);
+        cfg.dynamicSmemBytes = p->adj_smem;
+        cfg.stream = st;
+        cfg.attrs = &attr;
+        cfg.numAttrs = 1;
+        IMG2D_CUDA(cudaLaunchKernelEx(&cfg, p->adj_fn, a));
+    } else {
+        p->adj_fn<<<p->adj_grid, p->adj_block, p->adj_smem, st>>>(a);
+    }
     IMG2D_CUDA(cudaGetLastError());
     if (p->timing) {
         IMG2D_CUDA(cudaEventRecord(p->ev1, st));
@@ -1033,10 +1115,11 @@ int img2d_plan_describe_demigration(const img2d_plan *p, char *buf, int buflen)
     if (!p || !buf || buflen <= 0) return fail(IMG2D_EINVAL, "bad describe arguments");
     if (!p->adj_fn) return fail(IMG2D_EINVAL, "no demigration has run on this plan yet");
     snprintf(buf, buflen,
-             "{\"kernel\": \"demigrate\", \"G\": %d, \"X\": 8, \"L\": %d, \"grid\": %d, \"block\": %d, "
+             "{\"kernel\": \"%s\", \"cluster\": %d, \"G\": %d, \"X\": 8, \"L\": %d, \"grid\": %d, \"block\": %d, "
              "\"smem\": %zu, \"items\": %d, \"max_union_width\": %d, \"slab\": %d, \"slabs\": %d, "
              "\"workspace_bytes\": %zu, \"source_cache_bytes\": %zu}",
-             p->adj_G, p->L, p->adj_grid, p->adj_block, p->adj_smem, p->adj_items_n, p->adj_wmax, p->adj_slab,
+             p->adj_cluster ? "demigrate_cluster" : "demigrate", p->adj_cluster, p->adj_G, p->L, p->adj_grid,
+             p->adj_block, p->adj_smem, p->adj_items_n, p->adj_wmax, p->adj_slab,
              p->adj_nslab, p->adj_work.bytes, p->adj_cache.bytes);
     return IMG2D_OK;
 }

@@ -184,3 +184,44 @@ def test_source_checkpoint_modes_agree(case, slab):
     with pytest.raises(LibraryError, match="kept source checkpoints"):
         plan.demigrate(m, op.wave, op.zeros_data(), slab_depth=slab, source="reuse")
     plan.close()
+
+
+CLUSTER_CASES = {
+    "cluster_full_L31": lambda: synthetic.plain_medium(nx=700, nz=12, nf=4, ns=16),
+    "cluster_uneven_L35": lambda: synthetic.batched_uneven(nx=1300, nz=9, nf=3, ns=64),
+    "cluster_runtime_L11": lambda: _with_M(synthetic.plain_medium(nx=600, nz=8, nf=3, ns=14), 5),
+}
+
+
+@pytest.mark.parametrize("case", list(CLUSTER_CASES))
+@pytest.mark.parametrize("slab", [0, 3])
+def test_cluster_demigration_matches_oracle_and_single_cta(case, slab):
+    """The cluster demigration kernel (16 slots per item, window split over CTAs with halos in
+    distributed shared memory) against the FP64 oracle, and bit for bit against the single-CTA
+    kernel (same arithmetic per slot in the same order), in every source-checkpoint mode."""
+    import torch
+    w = CLUSTER_CASES[case]()
+    m = torch.from_numpy(np.random.default_rng(8).standard_normal((w.nextrap, w.nx)).astype(np.float32)).cuda()
+    op = _op(w, slab)
+    data = {}
+    for mode in ("recompute", "keep", "reuse"):
+        d = op.zeros_data()
+        op.plan.demigrate(m, op.wave, d, slab_depth=slab, source=mode)
+        data[mode] = d.cpu().numpy()
+    desc = op.plan.describe_demigration()
+    assert desc["kernel"] == "demigrate_cluster" and desc["G"] == 16, desc
+    if w.nx > 512:
+        assert desc["cluster"] >= 2, desc
+    single = lsm.MigrationOperator.for_workload(w, slab_depth=slab, no_cluster=True)
+    d1 = single.zeros_data()
+    single.plan.demigrate(m, single.wave, d1, slab_depth=slab, source="recompute")
+    assert single.plan.describe_demigration()["kernel"] == "demigrate"
+    ref = oracle.demigrate_workload_f64(w, m.cpu().numpy().astype(np.float64))
+    assert rel_l2(data["recompute"], ref) <= 1e-5
+    for mode in ("keep", "reuse"):
+        assert np.array_equal(data[mode], data["recompute"]), mode
+    assert np.array_equal(data["recompute"], d1.cpu().numpy())
+    lhs, rhs, rel, rel_norms = lsm.dot_product_test(op, seed=2)
+    assert rel_norms <= 1e-6 and rel <= 2e-5, (lhs, rhs, rel, rel_norms)
+    op.plan.close()
+    single.plan.close()
