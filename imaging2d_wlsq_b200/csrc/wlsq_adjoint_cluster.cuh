@@ -270,7 +270,9 @@ __global__ void __launch_bounds__(kDcNW * 32, 1) demigrate_cluster_kernel(Demigr
         // Phase 1: checkpoints S_{cD} (skipped when they come from the cache)
         if (a.ckpt_mode != 2) {
             for (int c = 0; c < a.nslab; ++c) {
-                for (int e = threadIdx.x; e < PC * Q; e += blockDim.x) ckpt[(long long)c * pe + e] = bufA[MP * Q + e];
+                // checkpoints are read once, a slab sweep later: evict-first in L2, so that the slab
+                // planes (re-read within D steps) keep their L2 lines
+                for (int e = threadIdx.x; e < PC * Q; e += blockDim.x) __stcs(ckpt + (long long)c * pe + e, bufA[MP * Q + e]);
                 if (c == a.nslab - 1) break;
                 for (int l = c * D; l < (c + 1) * D; ++l) forward_step(l, nullptr, l + 1);
             }
@@ -282,7 +284,7 @@ __global__ void __launch_bounds__(kDcNW * 32, 1) demigrate_cluster_kernel(Demigr
             const int lb = c * D;
             const int le = lb + D < a.nextrap ? lb + D : a.nextrap;
             if (c != a.nslab - 1 || a.ckpt_mode == 2) {
-                for (int e = threadIdx.x; e < PC * Q; e += blockDim.x) bufA[MP * Q + e] = ckpt[(long long)c * pe + e];
+                for (int e = threadIdx.x; e < PC * Q; e += blockDim.x) bufA[MP * Q + e] = __ldcs(ckpt + (long long)c * pe + e);
                 __syncthreads();
                 exchange(bufA);
             }

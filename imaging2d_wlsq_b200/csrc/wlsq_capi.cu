@@ -1272,14 +1272,17 @@ int img2d_records_to_spectra(int ns, int nt, int nx, int nf, int nt_rows, const 
     }
     const cufftHandle plan = itp->second;
     if (cufftSetStream(plan, st) != CUFFT_SUCCESS) return fail(IMG2D_ECUDA, "cufftSetStream failed");
+    // the spectra scratch (up to 512 MB) is kept per device with the plans, grown on demand
+    static std::map<int, DevBuf> spec_scratch;
+    DevBuf &spec = spec_scratch[dev];
+    if ((rc = spec.ensure((size_t)group * shot_spec * sizeof(cpx)))) return rc;
+    cpx *d_spec = spec.as<cpx>();
     Scratch sc;
     int *d_x0, *d_w;
     long long *d_off;
-    cpx *d_spec;
     if ((rc = sc.alloc(&d_x0, ns * sizeof(int)))) return rc;
     if ((rc = sc.alloc(&d_w, ns * sizeof(int)))) return rc;
     if ((rc = sc.alloc(&d_off, ns * sizeof(long long)))) return rc;
-    if ((rc = sc.alloc(&d_spec, (size_t)group * shot_spec * sizeof(cpx)))) return rc;
     IMG2D_CUDA(cudaMemcpyAsync(d_x0, x0.data(), ns * sizeof(int), cudaMemcpyHostToDevice, st));
     IMG2D_CUDA(cudaMemcpyAsync(d_w, w.data(), ns * sizeof(int), cudaMemcpyHostToDevice, st));
     IMG2D_CUDA(cudaMemcpyAsync(d_off, off.data(), ns * sizeof(long long), cudaMemcpyHostToDevice, st));
@@ -1295,7 +1298,7 @@ int img2d_records_to_spectra(int ns, int nt, int nx, int nf, int nt_rows, const 
         pack_spectra_kernel<<<blocks, 256, 0, st>>>(s0, nsc, nt, nx, nf, d_spec, d_x0, d_w, d_off, (cpx *)d_out);
         IMG2D_CUDA(cudaGetLastError());
     }
-    IMG2D_CUDA(cudaStreamSynchronize(st));  // descriptors and spectra scratch are freed on return
+    IMG2D_CUDA(cudaStreamSynchronize(st));  // the descriptors are freed on return
     return IMG2D_OK;
 }
 
