@@ -103,6 +103,8 @@ def load():
     lib.img2d_plan_demigrate.argtypes = [c_void_p] * 4 + [c_int, c_int, c_void_p]
     lib.img2d_plan_describe_demigration.restype = c_int
     lib.img2d_plan_describe_demigration.argtypes = [c_void_p, c_char_p, c_int]
+    lib.img2d_release_host_cache.restype = None
+    lib.img2d_release_host_cache.argtypes = []
     lib.img2d_plan_destroy.restype = None
     lib.img2d_plan_destroy.argtypes = [c_void_p]
     return lib

@@ -937,10 +937,16 @@ static int run_dense(int ns, int nextrap, int nz, int nx, int nf, int nt, int M,
     return IMG2D_OK;
 }
 
-// One cached plan for the host compact entry point, reused while the geometry is unchanged.
+// One cached plan for the host compact entry point, reused while the geometry is unchanged, and
+// its device buffers, kept between calls (grown on demand) so a call allocates nothing when the
+// sizes repeat.
 static std::mutex g_cache_mu;
 static img2d_plan *g_cached = nullptr;
 static std::vector<int> g_cached_key;
+struct HostEntryBuffers {
+    DevBuf omega, vel, tabF, tabB, wave, shot, image, image_shots;
+};
+static HostEntryBuffers *g_host_bufs = nullptr;
 
 }  // namespace img2d
 
@@ -1409,6 +1415,16 @@ int img2d_migrate_compact_noalloc(int ns, int nextrap, int nz, int nx, int nf, i
     return launch(&plan, a, d_image, nullptr, 0, st);
 }
 
+void img2d_release_host_cache(void)
+{
+    std::lock_guard<std::mutex> lock(g_cache_mu);
+    delete g_cached;
+    g_cached = nullptr;
+    g_cached_key.clear();
+    delete g_host_bufs;
+    g_host_bufs = nullptr;
+}
+
 int img2d_migrate_compact(int ns, int nextrap, int nz, int nx, int nf, int nt, int M, int nk, double dk,
                           const double *omega, const double *velocity, const img2d_c64 *tab_forw,
                           const img2d_c64 *tab_back, const int *shot_x0, const int *shot_nx,
@@ -1435,20 +1451,22 @@ int img2d_migrate_compact(int ns, int nextrap, int nz, int nx, int nf, int nt, i
         g_cached_key = key;
     }
     img2d_plan *p = g_cached;
-    Scratch sc;
+    if (!g_host_bufs) g_host_bufs = new HostEntryBuffers();
+    HostEntryBuffers &hb = *g_host_bufs;
     const size_t L = 2 * (size_t)M + 1;
     const size_t plane = (size_t)nz * nx;
-    double *dO, *dV;
-    cpx *dTF, *dTB = nullptr, *dW, *dS;
-    float *dI = nullptr, *dIS = nullptr;
-    if ((rc = sc.alloc(&dO, nf * sizeof(double)))) return rc;
-    if ((rc = sc.alloc(&dV, (size_t)nextrap * nx * sizeof(double)))) return rc;
-    if ((rc = sc.alloc(&dTF, nk * L * sizeof(cpx)))) return rc;
-    if ((flags & IMG2D_FLAG_TWO_TABLES) && (rc = sc.alloc(&dTB, nk * L * sizeof(cpx)))) return rc;
-    if ((rc = sc.alloc(&dW, p->wave_elems * sizeof(cpx)))) return rc;
-    if ((rc = sc.alloc(&dS, p->wave_elems * sizeof(cpx)))) return rc;
-    if (image && (rc = sc.alloc(&dI, (size_t)nextrap * nx * sizeof(float)))) return rc;
-    if (image_shots && (rc = sc.alloc(&dIS, (size_t)ns * plane * sizeof(float)))) return rc;
+    if ((rc = hb.omega.ensure(nf * sizeof(double)))) return rc;
+    if ((rc = hb.vel.ensure((size_t)nextrap * nx * sizeof(double)))) return rc;
+    if ((rc = hb.tabF.ensure(nk * L * sizeof(cpx)))) return rc;
+    if ((flags & IMG2D_FLAG_TWO_TABLES) && (rc = hb.tabB.ensure(nk * L * sizeof(cpx)))) return rc;
+    if ((rc = hb.wave.ensure(p->wave_elems * sizeof(cpx)))) return rc;
+    if ((rc = hb.shot.ensure(p->wave_elems * sizeof(cpx)))) return rc;
+    if (image && (rc = hb.image.ensure((size_t)nextrap * nx * sizeof(float)))) return rc;
+    if (image_shots && (rc = hb.image_shots.ensure((size_t)ns * plane * sizeof(float)))) return rc;
+    double *dO = hb.omega.as<double>(), *dV = hb.vel.as<double>();
+    cpx *dTF = hb.tabF.as<cpx>(), *dTB = (flags & IMG2D_FLAG_TWO_TABLES) ? hb.tabB.as<cpx>() : nullptr;
+    cpx *dW = hb.wave.as<cpx>(), *dS = hb.shot.as<cpx>();
+    float *dI = image ? hb.image.as<float>() : nullptr, *dIS = image_shots ? hb.image_shots.as<float>() : nullptr;
     IMG2D_CUDA(cudaMemcpy(dO, omega, nf * sizeof(double), cudaMemcpyHostToDevice));
     IMG2D_CUDA(cudaMemcpy(dV, velocity, (size_t)nextrap * nx * sizeof(double), cudaMemcpyHostToDevice));
     IMG2D_CUDA(cudaMemcpy(dTF, tab_forw, nk * L * sizeof(cpx), cudaMemcpyHostToDevice));

@@ -91,6 +91,9 @@ int img2d_migrate_compact(int ns, int nextrap, int nz, int nx, int nf, int nt, i
                           const img2d_c64 *tab_forw, const img2d_c64 *tab_back,
                           const int *shot_x0, const int *shot_nx, img2d_c64 *wave_fs,
                           img2d_c64 *shot_fs, float *image, float *image_shots, int flags);
+/* img2d_migrate_compact keeps its plan (for the last geometry) and its device buffers (grown to the
+ * largest sizes seen) between calls, so repeated calls allocate nothing.  This frees them. */
+void img2d_release_host_cache(void);
 
 /* ------------------------------------------------------------------------------------------
  * Plan interface for device-resident data (the building block under the host entry points).
