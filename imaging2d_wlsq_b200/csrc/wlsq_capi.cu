@@ -381,6 +381,40 @@ static int check_device()
     return IMG2D_OK;
 }
 
+// Largest portable cluster is 8 CTAs; B200 runs up to 16 when the kernel opts in.
+constexpr int kMaxCluster = 16;
+
+// How many clusters of K CTAs (block threads, smem bytes each) of `fn` fit on the device at once;
+// 0 when none does.  K > 8 sets the non-portable cluster-size attribute first.
+static int clusters_that_fit(const void *fn, int K, int block, size_t smem)
+{
+    if (K > 8 && cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    cudaLaunchConfig_t cfg{};
+    cudaLaunchAttribute attr{};
+    attr.id = cudaLaunchAttributeClusterDimension;
+    attr.val.clusterDim.x = K;
+    attr.val.clusterDim.y = 1;
+    attr.val.clusterDim.z = 1;
+    cfg.gridDim = dim3(K * 64, 1, 1);
+    cfg.blockDim = dim3(block, 1, 1);
+    cfg.dynamicSmemBytes = smem;
+    cfg.attrs = &attr;
+    cfg.numAttrs = 1;
+    int n = 0;
+    if (cudaOccupancyMaxActiveClusters(&n, fn, &cfg) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return n;
+}
+
 // Shared memory bytes of one CTA for groups of G shots over a union window of width W.
 static size_t smem_bytes(int G, int W, int M, int X)
 {
@@ -529,7 +563,7 @@ static int build_plan(img2d_plan *p, int ns, int nextrap, int nz, int nx, int nf
     if (cluster_ok && !(flags & IMG2D_FLAG_CLUSTER_V1) && p->L >= 7 && smem2 + static_reserve <= (size_t)smem_optin) {
         const int widest = make_groups(16);
         const int K = (widest + pc2 - 1) / pc2;
-        if (K <= 8) {
+        if (K <= 8 || (K <= kMaxCluster && clusters_that_fit((const void *)cv.fn, K, cv.nw * 32, smem2) > 0)) {
             p->cluster = K;
             p->G = 16;
             p->fixed = true;
@@ -543,7 +577,7 @@ static int build_plan(img2d_plan *p, int ns, int nextrap, int nz, int nx, int nf
     }
     if (tab16 && !p->cluster)
         return fail(IMG2D_EINVAL, "16-bit operator tables need the cluster kernel (>= 12 lane slots, 2M+1 >= 7, "
-                                  "window <= 8 CTAs)");
+                                  "window <= 16 CTAs)");
     p->tab16 = tab16;
     const ClusterKernel *ck = cluster_ok ? find_cluster(p->L) : nullptr;
     if (!p->cluster && ck && ck->smem + static_reserve <= (size_t)smem_optin) {
@@ -790,7 +824,9 @@ static int demig_prepare(img2d_plan *p, int slab)
         demigc_smem_bytes(p->M) + static_reserve <= (size_t)smem_optin) {
         widest = pack_groups(p, 16, groups, segs, owner);
         const int k = (widest + kDcPC - 1) / kDcPC;
-        if (k <= 8) {
+        DemigFn cfn = find_demig_cluster(p->L);
+        if (k <= 8 || (k <= kMaxCluster && cfn &&
+                       clusters_that_fit((const void *)cfn, k, kDcNW * 32, demigc_smem_bytes(p->M)) > 0)) {
             K = k;
             G = 16;
             fn = find_demig_cluster(p->L);

@@ -225,3 +225,15 @@ def test_cluster_demigration_matches_oracle_and_single_cta(case, slab):
     assert rel_norms <= 1e-6 and rel <= 2e-5, (lhs, rhs, rel, rel_norms)
     op.plan.close()
     single.plan.close()
+
+
+def test_wide_window_non_portable_cluster_demigration():
+    import torch
+    w = synthetic.plain_medium(nx=6000, nz=4, nf=2, ns=12)
+    op = _op(w)
+    m = torch.from_numpy(np.random.default_rng(9).standard_normal((w.nextrap, w.nx)).astype(np.float32)).cuda()
+    data = op.demigrate(m).cpu().numpy()
+    desc = op.plan.describe_demigration()
+    assert desc["kernel"] == "demigrate_cluster" and desc["cluster"] == 12, desc
+    assert rel_l2(data, oracle.demigrate_workload_f64(w, m.cpu().numpy().astype(np.float64))) <= 1e-5
+    op.plan.close()

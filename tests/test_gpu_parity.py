@@ -275,3 +275,13 @@ def test_staged_default_matches_unstaged_bitwise():
     assert np.array_equal(wave0, wave1) and np.array_equal(shot0, shot1)
     assert rel_l2(img0, img1) <= 1e-6
     _compact_check(w, img0, wave0, shot0)
+
+
+def test_wide_window_non_portable_cluster():
+    """A 6000-position full-aperture window needs 12 CTAs of 512 positions: a non-portable cluster
+    size (up to 16 on B200 with the kernel's opt-in)."""
+    w = synthetic.plain_medium(nx=6000, nz=4, nf=2, ns=12)
+    d = migration.Plan.for_workload(w).describe()
+    assert d["kernel"] == "migrate_cluster2" and d["cluster"] == 12, d
+    img, _, wave, shot = migration.migrate_workload(w)
+    _compact_check(w, img, wave, shot)
