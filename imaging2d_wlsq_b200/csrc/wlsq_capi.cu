@@ -931,10 +931,37 @@ struct Scratch {
 };
 
 // Dense-table drop-in: both argument orders come here.
+// Sizes for which the reference's loops (cpp_src/extrapolation_cpu.cpp:39-99) do no extrapolation:
+// ns, nx or nextrap zero leave every buffer as it was; nf zero writes zero image rows [0, nextrap).
+// Handled on the host; returns 1 when the call is complete.
+static int degenerate_call(int ns, int nextrap, int nz, int nx, int nf, float *image, int *rc)
+{
+    if (ns < 0 || nextrap < 0 || nz < 0 || nx < 0 || nf < 0 || nz < nextrap) {
+        *rc = fail(IMG2D_EINVAL, "invalid dimensions (negative, or nz < nextrap)");
+        return 1;
+    }
+    if (ns == 0 || nx == 0 || nextrap == 0) {
+        *rc = IMG2D_OK;
+        return 1;
+    }
+    if (nf == 0) {
+        if (!image) {
+            *rc = fail(IMG2D_EINVAL, "null image pointer");
+            return 1;
+        }
+        for (int s = 0; s < ns; ++s)
+            std::memset(image + (size_t)s * nz * nx, 0, (size_t)nextrap * nx * sizeof(float));
+        *rc = IMG2D_OK;
+        return 1;
+    }
+    return 0;
+}
+
 static int run_dense(int ns, int nextrap, int nz, int nx, int nf, int nt, int M, const cpx *opF,
                      const cpx *opB, cpx *wave, cpx *shot, float *image, int write_back)
 {
     int rc;
+    if (degenerate_call(ns, nextrap, nz, nx, nf, image, &rc)) return rc;
     if ((rc = check_device())) return rc;
     if (!opF || !opB || !wave || !shot || !image) return fail(IMG2D_EINVAL, "null pointer argument");
     img2d_plan plan;

@@ -69,3 +69,36 @@ def test_no_device_reports_enodev():
 
 def test_version():
     assert _lib.lib().img2d_version() >= 10000
+
+
+@pytest.mark.parametrize("dims", [dict(ns=0, nextrap=2, nf=2), dict(ns=2, nextrap=0, nf=2),
+                                  dict(ns=2, nextrap=2, nf=0)], ids=["ns0", "nextrap0", "nf0"])
+def test_degenerate_sizes_behave_like_reference(dims):
+    """Sizes for which the reference's loops do no extrapolation (no shots, no depth steps, no
+    frequencies) leave the buffers as the reference's own CPU library does (nf = 0 writes zero
+    image rows); no GPU is needed."""
+    from oracle import oracle
+    from imaging2d_wlsq_b200 import interface, interface_cuda
+    ns, nextrap, nf = dims["ns"], dims["nextrap"], dims["nf"]
+    nz, nx, nt, M = 3, 5, 3, 1
+    rng = np.random.default_rng(1)
+    op = (rng.standard_normal((max(nextrap, 1), max(nf, 1), nx, 3)) + 0j).astype(np.complex64)
+    wave = (rng.standard_normal((max(ns, 1), nt, nx)) + 1j).astype(np.complex64)
+    shot = (rng.standard_normal((max(ns, 1), nt, nx)) - 1j).astype(np.complex64)
+    img0 = np.full((max(ns, 1), nz, nx), 7.0, dtype=np.float32)
+    outs = []
+    calls = [lambda w, s, i: interface.extrapolate(ns, nextrap, nz, nx, nf, nt, M, op, op, w, s, i),
+             lambda w, s, i: interface_cuda.extrapolate_revOp(ns, nextrap, nz, nt, nf, nx, M, op, w, op, s, i)]
+    if oracle.have_ref():
+        calls.append(lambda w, s, i: oracle.ref_extrapolate(ns, nextrap, nz, nx, nf, nt, M, op, op, w, s, i))
+    for call in calls:
+        w, s, i = wave.copy(), shot.copy(), img0.copy()
+        call(w, s, i)
+        outs.append((w, s, i))
+    for w, s, i in outs:
+        np.testing.assert_array_equal(w, wave)
+        np.testing.assert_array_equal(s, shot)
+        expect = img0.copy()
+        if nf == 0:
+            expect[:ns, :nextrap] = 0.0
+        np.testing.assert_array_equal(i, expect)
