@@ -106,6 +106,7 @@ struct Cluster2Variant {
     bool tap_pf, row_pf;
     KernelFn fn;
     bool stage = false;  // uses the step-ahead shared-memory stage (cluster2_stage_bytes)
+    bool ring = false;   // reads operator taps from the per-lane-group ring (cluster2_ring_bytes)
 };
 
 static const Cluster2Variant kCluster2[] = {
@@ -120,6 +121,7 @@ static const Cluster2Variant kCluster2[] = {
     {16, false, false, migrate_cluster2_kernel<16, false, false, false, TAB_F32, 2>},  // index prefetch
     {16, false, false, migrate_cluster2_kernel<16, false, false, false, TAB_F32, 3>},  // both
     {16, false, false, migrate_cluster2_kernel<16, false, false, false, TAB_F32, 4>, true},  // step-ahead stage
+    {16, false, false, migrate_cluster2_kernel<16, false, false, false, TAB_F32, 8>, false, true},  // tap-pair ring
 };
 constexpr int kCluster2Default = 10;  // 16 warps with the step-ahead shared-memory stage
 constexpr int kNumCluster2 = (int)(sizeof(kCluster2) / sizeof(kCluster2[0]));
@@ -538,10 +540,11 @@ static int build_plan(img2d_plan *p, int ns, int nextrap, int nz, int nx, int nf
     std::vector<int16_t> owner;
     auto make_groups = [&](int G) { return pack_groups(p, G, groups, segs, owner); };
 
-    // Kernel choice.  The cluster kernel (16 slots per item, 256 positions per CTA, up to 8 CTAs
-    // per cluster) when the operator length has an instance, there are enough slots to fill it
-    // and the widest group fits 8 CTAs; otherwise the single-CTA kernels with the largest power
-    // of two <= 8 slots whose ping-pong buffers fit in shared memory.
+    // Kernel choice.  The second-generation cluster kernel (16 slots per item, 512 positions per CTA,
+    // clusters of up to 16 CTAs where they fit) when there are enough slots to fill it and the
+    // operator has at least 7 taps; else the first-generation cluster kernel (256 positions per CTA,
+    // up to 8 CTAs, compile-time operator lengths); otherwise the single-CTA kernels with the
+    // largest power of two <= 8 slots whose ping-pong buffers fit in shared memory.
     p->cluster = 0;
     p->block = 256;
     const bool cluster_ok = mode == OP_CONJ && !(flags & (IMG2D_FLAG_GENERIC | IMG2D_FLAG_NO_CLUSTER)) &&
@@ -559,7 +562,8 @@ static int build_plan(img2d_plan *p, int ns, int nextrap, int nz, int nx, int nf
         vsel = kCluster2Default;
     }
     const int pc2 = cv.nw * 32;
-    const size_t smem2 = cluster2_smem_bytes(M, pc2) + (cv.stage ? cluster2_stage_bytes(pc2) : 0);
+    const size_t smem2 = cluster2_smem_bytes(M, pc2) + (cv.stage ? cluster2_stage_bytes(pc2) : 0) +
+                         (cv.ring ? cluster2_ring_bytes(pc2) : 0);
     if (cluster_ok && !(flags & IMG2D_FLAG_CLUSTER_V1) && p->L >= 7 && smem2 + static_reserve <= (size_t)smem_optin) {
         const int widest = make_groups(16);
         const int K = (widest + pc2 - 1) / pc2;

@@ -108,10 +108,24 @@ __device__ __forceinline__ void cp_async4(void *smem_dst, const void *gsrc)
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+// 16-byte global -> shared copy through L2 only (no L1 allocation)
+__device__ __forceinline__ void cp_async16(void *smem_dst, const void *gsrc)
+{
+    const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(gsrc) : "memory");
+}
+// wait until at most N of this thread's most recent commit groups are still in flight
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
 // Shared memory of the step-ahead stage (OPT bit 2): per parity, one 32-bit index word and the
 // Kahan partial and compensation values of every position of the CTA.
 __host__ __device__ inline size_t cluster2_stage_bytes(int pc) { return (size_t)pc * (2 * 4 + 2 * 2 * 4); }
+
+// Operator-pair ring (OPT bit 3): per lane group, kRingSlots 16-byte tap pairs of each of its X
+// output rows, plus one 16-byte pad per group so that the four groups of a warp read disjoint banks.
+constexpr int kRingSlots = 4;
+__host__ __device__ inline size_t cluster2_ring_bytes(int pc) { return (size_t)(pc / 8) * (8 * kRingSlots + 1) * 16; }
 
 // NWARPS: warps per CTA (positions per CTA = 32 * NWARPS).  TAP_PF: operator tap pairs are loaded one
 // step ahead into a second register set.  ROW_PF: the next depth step's operator rows are prefetched
@@ -119,7 +133,9 @@ __host__ __device__ inline size_t cluster2_stage_bytes(int pc) { return (size_t)
 // bit 1: the next depth step's operator indices are prefetched into L1 one step ahead; bit 2: the
 // next step's operator indices and Kahan partial-image rows are copied into shared memory
 // (cp.async) one step ahead, so neither the index loads at the start of a step nor the imaging
-// read-modify-write at its end waits on DRAM.
+// read-modify-write at its end waits on DRAM; bit 3 (instead of bit 2): the operator tap pairs reach
+// the tap loop through a per-lane-group shared-memory ring instead of L1, and the next step's
+// operator index and Kahan values come one step ahead in registers (see RING below).
 template <int NWARPS, bool TAP_PF, bool ROW_PF, bool PACKED = false, int TT = TAB_F32, int OPT = 0>
 __global__ void __launch_bounds__(NWARPS * 32, 1) migrate_cluster2_kernel(MigrateArgs a)
 {
@@ -127,6 +143,20 @@ __global__ void __launch_bounds__(NWARPS * 32, 1) migrate_cluster2_kernel(Migrat
     constexpr int Q = S::Q, G = S::G, P = S::P, X = S::X, PC = S::PC;
     constexpr bool STAGE = (OPT & 4) != 0;
     static_assert(!STAGE || Q == X, "the stage gives lane q of a group position q of its block");
+    // RING: lane q of a lane group owns output q of the group's block.  It copies the tap pairs of
+    // that output's operator row into the group's shared-memory ring with 16-byte cp.async through
+    // L2, three tap-loop iterations before they are read, so the tap loop reads its operator taps
+    // from shared memory instead of waiting on L1 sector misses.  Output jj reads its pair p at
+    // iteration u = p - (X - jj) / 2 of the tap loop (the prologue has u < 0, the middle loop
+    // u = 0 .. nmid-1, the epilogue u = nmid .. nmid+3) from ring slot u mod 4, so all outputs of the
+    // group read slot u mod 4 at iteration u, and one commit group per iteration lets the loop wait
+    // for exactly the pairs it is about to read.  The pairs with u < 0 are copied at the end of the
+    // previous depth step.  The next step's operator index and Kahan partial-image values of the
+    // lane's own position are loaded into registers one step ahead; lane q also does the Kahan
+    // update of its position, so no other staging is needed.
+    constexpr bool RING = (OPT & 8) != 0;
+    static_assert(!RING || (!STAGE && TT == TAB_F32 && !TAP_PF && !ROW_PF && !PACKED && Q == X && X == 8),
+                  "the ring variant is built on the 16-byte FP32 tap loop with lane q owning output q");
     const int M = a.M, L = 2 * a.M + 1;
     const int MP = cluster2_mp(M);
     const int NEXT = PC + 2 * MP;
@@ -148,6 +178,9 @@ __global__ void __launch_bounds__(NWARPS * 32, 1) migrate_cluster2_kernel(Migrat
     float *cmp = a.comp ? a.comp + (long long)blockIdx.x * a.nextrap * a.nx : nullptr;
     const bool push_left = crank > 0 && b * X < MP;
     const bool push_right = crank + 1 < csize && b * X + X > PC - MP;
+    // RING: this lane group's ring, [output][slot] float4 plus one pad, after the halo staging
+    float4 *const ringb = smem + (size_t)(NEXT + 4 * MP) * G + (size_t)b * (X * kRingSlots + 1);
+    const int npairs = (L + 1) >> 1, cq = (X - q) >> 1;
     const unsigned rank0_item = map_rank(&s_item, 0);
     // row r starts at byte r * row_bytes; taps are addressed in pairs through load_tap_pair
     const char *tabb = reinterpret_cast<const char *>(TT == TAB_F32 ? (const void *)a.tabF : a.tab16);
@@ -203,7 +236,7 @@ __global__ void __launch_bounds__(NWARPS * 32, 1) migrate_cluster2_kernel(Migrat
         const uint16_t *idx_j = a.idx + (long long)j * a.idx_jstride;
         const int xg = u0 + c0 + b * X;  // model position of the block's first output
         const bool img_lane = part && q == 0 && blk_active;
-        if (img_lane && !STAGE) {
+        if (img_lane && !STAGE && !RING) {
             asm volatile("prefetch.global.L1 [%0];" ::"l"(part + xg));
             asm volatile("prefetch.global.L1 [%0];" ::"l"(cmp + xg));
         }
@@ -225,6 +258,26 @@ __global__ void __launch_bounds__(NWARPS * 32, 1) migrate_cluster2_kernel(Migrat
             cp_async_commit();
         };
         if (STAGE) stage_step(0);
+        // RING state of the lane's own position xg + q: its operator row at the current step, its
+        // row index at the next step, and the Kahan partial/compensation values of both steps
+        const uint16_t *idx_q = idx_j + xq;
+        const char *row_q = tabb;
+        unsigned nidx = 0;
+        float cur_s = 0.f, cur_c = 0.f, nxt_s = 0.f, nxt_c = 0.f;
+        auto ring_copy = [&](int u) {
+            const int pr = u + cq;
+            if (pr >= 0 && pr < npairs)
+                cp_async16(ringb + q * kRingSlots + (u & (kRingSlots - 1)), row_q + (size_t)pr * 16);
+        };
+        if (RING) {
+            row_q = tabb + (size_t)idx_q[0] * row_bytes;
+            for (int u = -(X / 2); u < 0; ++u) ring_copy(u);
+            cp_async_commit();
+            if (stage_img) {
+                nxt_s = part[xg + q];
+                nxt_c = cmp[xg + q];
+            }
+        }
 
         for (int l = 0; l < a.nextrap; ++l) {
             const int par = l & 1;
@@ -241,6 +294,19 @@ __global__ void __launch_bounds__(NWARPS * 32, 1) migrate_cluster2_kernel(Migrat
                     roff[jj] = (int)((wv >> (16 * (xj & 1))) & 0xffffu) * row_bytes;
                 }
                 stage_step(l + 1);
+            } else if (RING) {
+                // this step's prologue pairs (copied at the end of the previous step) for the group
+                cp_async_wait_all();
+                __syncwarp(gmask);
+                cur_s = nxt_s;
+                cur_c = nxt_c;
+                if (l + 1 < a.nextrap) {
+                    nidx = idx_q[(long long)(l + 1) * a.idx_lstride];
+                    if (stage_img) {
+                        nxt_s = part[(long long)(l + 1) * a.nx + xg + q];
+                        nxt_c = cmp[(long long)(l + 1) * a.nx + xg + q];
+                    }
+                }
             } else {
 #pragma unroll
                 for (int jj = 0; jj < X; ++jj) roff[jj] = (int)idx_l[min(xg + jj, a.nx - 1)] * row_bytes;
@@ -253,7 +319,7 @@ __global__ void __launch_bounds__(NWARPS * 32, 1) migrate_cluster2_kernel(Migrat
             }
             if ((OPT & 2) && q == 0 && l + 1 < a.nextrap)
                 asm volatile("prefetch.global.L1 [%0];" ::"l"(idx_l + a.idx_lstride + min(xg, a.nx - 1)));
-            if (img_lane && !STAGE && l + 1 < a.nextrap) {
+            if (img_lane && !STAGE && !RING && l + 1 < a.nextrap) {
                 asm volatile("prefetch.global.L1 [%0];" ::"l"(part + (long long)(l + 1) * a.nx + xg));
                 asm volatile("prefetch.global.L1 [%0];" ::"l"(cmp + (long long)(l + 1) * a.nx + xg));
             }
@@ -279,11 +345,18 @@ __global__ void __launch_bounds__(NWARPS * 32, 1) migrate_cluster2_kernel(Migrat
                 for (int jj = 0; jj < X; ++jj) {
                     const int k = t - jj;
                     if (k >= 0) {
-                        if ((k & 1) == 0) tp[jj] = load_tap_pair<TT>(tabb + roff[jj], (k >> 1));
+                        if ((k & 1) == 0)
+                            tp[jj] = RING ? ringb[jj * kRingSlots + (((k >> 1) - ((X - jj) >> 1)) & (kRingSlots - 1))]
+                                          : load_tap_pair<TT>(tabb + roff[jj], (k >> 1));
                         const float fr = (k & 1) ? tp[jj].z : tp[jj].x;
                         const float fi = (k & 1) ? tp[jj].w : tp[jj].y;
                         IMG2D_MAC(acc[jj], fr, fi, va, vb);
                     }
+                }
+                // RING: after t = 2u the slot of iteration u - 4 has been read; copy iteration u
+                if (RING && (t & 1) == 0 && (t >> 1) < 3) {
+                    ring_copy(t >> 1);
+                    cp_async_commit();
                 }
             }
             // middle: t = X-1 .. L-1 in steps of two (odd t, then even t+1)
@@ -292,6 +365,14 @@ __global__ void __launch_bounds__(NWARPS * 32, 1) migrate_cluster2_kernel(Migrat
             if (!TAP_PF) {
                 int kbase = X - 1;  // k of output 0 at the odd step
                 for (int u = 0; u < nmid; ++u, sp += 2 * G, kbase += 2) {
+                    const float4 *rs = ringb + (u & (kRingSlots - 1));
+                    if (RING) {
+                        // iteration u - 1 has read the slot of iteration u + 3; wait for iteration u
+                        ring_copy(u + 3);
+                        cp_async_commit();
+                        cp_async_wait<3>();
+                        __syncwarp(gmask);
+                    }
                     {
                         const float4 va = sp[0];
                         const float4 vb = sp[Q];
@@ -300,7 +381,8 @@ __global__ void __launch_bounds__(NWARPS * 32, 1) migrate_cluster2_kernel(Migrat
 #pragma unroll
                         for (int jj = 0; jj < X; ++jj) {
                             // k = kbase - jj: even for odd jj (new pair), odd for even jj (held pair)
-                            if (jj & 1) tp[jj] = load_tap_pair<TT>(tabb + roff[jj], ((kbase - jj) >> 1));
+                            if (jj & 1)
+                                tp[jj] = RING ? rs[jj * kRingSlots] : load_tap_pair<TT>(tabb + roff[jj], ((kbase - jj) >> 1));
                             const float fr = (jj & 1) ? tp[jj].x : tp[jj].z;
                             const float fi = (jj & 1) ? tp[jj].y : tp[jj].w;
                             if (PACKED) IMG2D_MAC8P(acc[jj], fr, fi, va, vb, swa0, swa1, swb0, swb1);
@@ -314,7 +396,9 @@ __global__ void __launch_bounds__(NWARPS * 32, 1) migrate_cluster2_kernel(Migrat
                         const float2 swb0 = make_float2(vb.y, vb.x), swb1 = make_float2(vb.w, vb.z);
 #pragma unroll
                         for (int jj = 0; jj < X; ++jj) {
-                            if (!(jj & 1)) tp[jj] = load_tap_pair<TT>(tabb + roff[jj], ((kbase + 1 - jj) >> 1));
+                            if (!(jj & 1))
+                                tp[jj] = RING ? rs[jj * kRingSlots]
+                                              : load_tap_pair<TT>(tabb + roff[jj], ((kbase + 1 - jj) >> 1));
                             const float fr = (jj & 1) ? tp[jj].z : tp[jj].x;
                             const float fi = (jj & 1) ? tp[jj].w : tp[jj].y;
                             if (PACKED) IMG2D_MAC8P(acc[jj], fr, fi, va, vb, swa0, swa1, swb0, swb1);
@@ -367,16 +451,32 @@ __global__ void __launch_bounds__(NWARPS * 32, 1) migrate_cluster2_kernel(Migrat
             }
             // epilogue: t = L .. L+X-2, outputs jj > t-L are active (k = t - jj <= L-1)
             const float4 *ep = src + (size_t)L * G;
+            if (RING) {
+                ring_copy(nmid + 3);
+                cp_async_commit();
+            }
 #pragma unroll
             for (int e = 0; e < X - 1; ++e) {
                 const float4 va = ep[(size_t)e * G];
                 const float4 vb = ep[(size_t)e * G + Q];
+                if (RING && (e & 1) == 0) {
+                    // steps e and e + 1 read iteration nmid + e / 2; later iterations may be in flight
+                    switch (e >> 1) {
+                        case 0: cp_async_wait<3>(); break;
+                        case 1: cp_async_wait<2>(); break;
+                        case 2: cp_async_wait<1>(); break;
+                        default: cp_async_wait<0>(); break;
+                    }
+                    __syncwarp(gmask);
+                }
 #pragma unroll
                 for (int jj = 0; jj < X; ++jj) {
                     if (jj > e) {
                         // k = L + e - jj, parity of (1 + e - jj) since L is odd
                         const bool even = ((1 + e - jj) & 1) == 0;
-                        if (even) tp[jj] = load_tap_pair<TT>(tabb + roff[jj], ((L + e - jj) >> 1));
+                        if (even)
+                            tp[jj] = RING ? ringb[jj * kRingSlots + ((nmid + (e >> 1)) & (kRingSlots - 1))]
+                                          : load_tap_pair<TT>(tabb + roff[jj], ((L + e - jj) >> 1));
                         const float fr = even ? tp[jj].x : tp[jj].z;
                         const float fi = even ? tp[jj].y : tp[jj].w;
                         IMG2D_MAC(acc[jj], fr, fi, va, vb);
@@ -387,6 +487,15 @@ __global__ void __launch_bounds__(NWARPS * 32, 1) migrate_cluster2_kernel(Migrat
             for (int jj = 0; jj < X; ++jj) {
                 if (!((in_a >> jj) & 1u)) acc[jj][0] = acc[jj][1] = acc[jj][2] = acc[jj][3] = 0.f;
                 if (!((in_b >> jj) & 1u)) acc[jj][4] = acc[jj][5] = acc[jj][6] = acc[jj][7] = 0.f;
+            }
+            if (RING) {
+                // every ring slot has been read: copy the next step's prologue pairs (u < 0) now, so
+                // that they arrive during the halo exchange and the imaging
+                if (l + 1 < a.nextrap) {
+                    row_q = tabb + (size_t)nidx * row_bytes;
+                    for (int u = -(X / 2); u < 0; ++u) ring_copy(u);
+                }
+                cp_async_commit();
             }
             // halos of step l+1 into the neighbours' staging (parity par^1); see wlsq_cluster.cuh
             if (push_left) {
@@ -423,6 +532,7 @@ __global__ void __launch_bounds__(NWARPS * 32, 1) migrate_cluster2_kernel(Migrat
             cluster_arrive();
             float *prow = part ? part + (long long)l * a.nx : nullptr;
             float *crow = cmp ? cmp + (long long)l * a.nx : nullptr;
+            float img_q = 0.f;  // RING: the stacked image value of the lane's own position
 #pragma unroll
             for (int jj = 0; jj < X; ++jj) {
                 const float ia = acc[jj][0] * acc[jj][2] - acc[jj][1] * acc[jj][3];
@@ -437,7 +547,9 @@ __global__ void __launch_bounds__(NWARPS * 32, 1) migrate_cluster2_kernel(Migrat
                 float img = ia + ib;
 #pragma unroll
                 for (int off = 1; off < Q; off <<= 1) img += __shfl_xor_sync(gmask, img, off);
-                if (prow && q == 0 && c0 + b * X + jj < W) {
+                if (RING) {
+                    if (jj == q) img_q = img;
+                } else if (prow && q == 0 && c0 + b * X + jj < W) {
                     if (STAGE) {
                         // kahan_add on the staged values; the stores need not be waited for
                         float sum = spart[(par * 2 + 0) * PC + b * X + jj];
@@ -451,6 +563,13 @@ __global__ void __launch_bounds__(NWARPS * 32, 1) migrate_cluster2_kernel(Migrat
                         kahan_add(prow + xg + jj, crow + xg + jj, img);
                     }
                 }
+            }
+            if (RING && stage_img) {
+                // kahan_add on the values loaded a step ahead (same operations as the other forms)
+                const float y = img_q - cur_c;
+                const float t = cur_s + y;
+                prow[xg + q] = t;
+                crow[xg + q] = (t - cur_s) - y;
             }
             cluster_wait();
             const float4 *hs = stg + (size_t)((par ^ 1) * 2) * MP * G;

@@ -163,8 +163,10 @@ class Plan:
 # ---------------------------------------------------------------------------------------------
 
 # Candidate kernel configurations, as Plan keyword arguments.  cluster2 variants differ in warps per
-# CTA (positions per CTA), operator-pair prefetch depth, L1 row prefetch and packed arithmetic.
-CANDIDATES = [("default", {})] + [("cluster2/v%d" % v, {"variant": v}) for v in range(1, 12)] + \
+# CTA (positions per CTA), operator-pair prefetch depth, L1 row prefetch, packed arithmetic, and how
+# operator indices, Kahan rows and tap pairs reach the tap loop (L1, shared-memory stage or ring).
+N_CLUSTER2_VARIANTS = 12
+CANDIDATES = [("default", {})] + [("cluster2/v%d" % v, {"variant": v}) for v in range(1, N_CLUSTER2_VARIANTS + 1)] + \
              [("cluster1", {"cluster_v1": True}), ("single-cta", {"no_cluster": True})]
 
 

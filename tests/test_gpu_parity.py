@@ -12,7 +12,7 @@ import numpy as np
 import pytest
 from numpy.ctypeslib import ndpointer
 
-from imaging2d_wlsq_b200 import DROPIN_DIR, interface, interface_cuda, migration, synthetic
+from imaging2d_wlsq_b200 import DROPIN_DIR, interface, interface_cuda, migration, operators, synthetic
 from oracle import oracle
 from tests import kat_cases as K
 from tests.conftest import rel_l2
@@ -244,7 +244,7 @@ def test_cluster_kernel_matches_oracle_and_single_cta(kind, nx, nz, nf, ns, v1):
     assert e <= 1e-5
 
 
-@pytest.mark.parametrize("variant", list(range(1, 12)))
+@pytest.mark.parametrize("variant", list(range(1, migration.N_CLUSTER2_VARIANTS + 1)))
 def test_cluster2_variants_match_oracle(variant):
     """Every variant of the second-generation cluster kernel (warps per CTA, operator-pair
     prefetch, L1 row prefetch) on a window that needs a multi-CTA cluster."""
@@ -275,6 +275,25 @@ def test_staged_default_matches_unstaged_bitwise():
     assert np.array_equal(wave0, wave1) and np.array_equal(shot0, shot1)
     assert rel_l2(img0, img1) <= 1e-6
     _compact_check(w, img0, wave0, shot0)
+
+
+def test_ring_variant_matches_default_bitwise():
+    """Variant 12 reads the operator tap pairs from a per-lane-group shared-memory ring filled by
+    16-byte cp.async copies and keeps the next step's index and Kahan values in registers; the tap
+    values and the FMA order are those of the default, so final wavefields are bit-identical.  Runs
+    an operator length with a middle loop (35 taps) and the shortest one without (7 taps)."""
+    for taps in (35, 7):
+        w = synthetic.batched_uneven(nx=1500, nz=9, nf=4, ns=48, scale=1.0)
+        if taps != 2 * w.M + 1:
+            w.M = (taps - 1) // 2
+            w.table = operators.design_compact_table(w.nx, w.dx, w.dz, w.M, w.nk, w.dk)
+        d = migration.Plan.for_workload(w, variant=12).describe()
+        assert d["kernel"] == "migrate_cluster2" and d["variant"] == 11, d
+        img0, _, wave0, shot0 = migration.migrate_workload(w)
+        img1, _, wave1, shot1 = migration.migrate_workload(w, variant=12)
+        assert np.array_equal(wave0, wave1) and np.array_equal(shot0, shot1), taps
+        assert rel_l2(img0, img1) <= 1e-6, taps
+        _compact_check(w, img1, wave1, shot1)
 
 
 def test_wide_window_non_portable_cluster():
