@@ -34,10 +34,9 @@ METRIC = "extrapolated pts/s (shot*w*z*x), batched vs plain on 1 GPU; rel-L2 err
 UNIT = "pts/s"
 
 
-# ncu, default migration kernel (variant index 10) on the full batched_uneven launch:
-# dram__bytes_read.sum 98.07 GB + dram__bytes_write.sum 78.56 GB
-DEFAULT_VARIANT_INDEX = 10
-PROFILED_TRAFFIC_BYTES = 176.63e9
+# ncu (dram__bytes_read.sum + dram__bytes_write.sum, one pass) of one full batched_uneven launch,
+# per cluster-kernel variant index: the staged variant 98.07 + 78.56 GB
+PROFILED_TRAFFIC_BYTES = {10: 176.63e9}
 
 
 def parse_args():
@@ -511,11 +510,13 @@ def main():
         # DRAM bytes of one launch of the default kernel on the full batched_uneven workload, from one
         # ncu capture (dram__bytes_read.sum + dram__bytes_write.sum, single pass); other shapes: null
         if (w.name == "batched_uneven" and args.scale == 1.0 and not (args.nz or args.nf or args.taps)
-                and describe.get("variant") == DEFAULT_VARIANT_INDEX and world == 1):
-            roof["traffic"] = PROFILED_TRAFFIC_BYTES
+                and describe.get("kernel") == "migrate_cluster2"
+                and describe.get("variant") in PROFILED_TRAFFIC_BYTES and world == 1):
+            traffic = PROFILED_TRAFFIC_BYTES[describe["variant"]]
+            roof["traffic"] = traffic
             roof["traffic_unit"] = "bytes per launch"
             roof["traffic_source"] = "profiles/migrate_cluster2_kernel_batched_uneven.md"
-            roof_hbm["traffic_gbs"] = PROFILED_TRAFFIC_BYTES / k_s / 1e9
+            roof_hbm["traffic_gbs"] = traffic / k_s / 1e9
         l2 = migration.l2_read_bandwidth_gbs()
         roof_l2 = {"bound": "l2", "achieved": ach_b, "peak": l2, "unit": "GB/s", "frac": ach_b / l2,
                    "per_point": f"{bytes_pt} B (8L operator bytes gathered per point)",

@@ -123,7 +123,8 @@ static const Cluster2Variant kCluster2[] = {
     {16, false, false, migrate_cluster2_kernel<16, false, false, false, TAB_F32, 4>, true},  // step-ahead stage
     {16, false, false, migrate_cluster2_kernel<16, false, false, false, TAB_F32, 8>, false, true},  // tap-pair ring
 };
-constexpr int kCluster2Default = 10;  // 16 warps with the step-ahead shared-memory stage
+constexpr int kCluster2Staged = 10;   // 16 warps with the step-ahead shared-memory stage
+constexpr int kCluster2Default = 11;  // 16 warps, tap pairs through the shared-memory ring
 constexpr int kNumCluster2 = (int)(sizeof(kCluster2) / sizeof(kCluster2[0]));
 
 // Demigration kernels: G lane slots per item, compile-time operator length (0 = runtime length).
@@ -550,34 +551,44 @@ static int build_plan(img2d_plan *p, int ns, int nextrap, int nz, int nx, int nf
     const bool cluster_ok = mode == OP_CONJ && !(flags & (IMG2D_FLAG_GENERIC | IMG2D_FLAG_NO_CLUSTER)) &&
                             p->n_slots >= 12;
     int vsel = (flags >> IMG2D_FLAG_VARIANT_SHIFT) & 0xff;
-    vsel = (vsel >= 1 && vsel <= kNumCluster2) ? vsel - 1 : kCluster2Default;
+    const bool explicit_variant = vsel >= 1 && vsel <= kNumCluster2;
+    vsel = explicit_variant ? vsel - 1 : kCluster2Default;
     Cluster2Variant cv = kCluster2[vsel];
     const int tab16 = (flags & IMG2D_FLAG_TABLE_BF16) ? 2 : ((flags & IMG2D_FLAG_TABLE_FP16) ? 1 : 0);
     if (tab16) {
-        // reduced-precision operator storage: default shape with 16-bit tap loads
+        // reduced-precision operator storage: the staged shape with 16-bit tap loads
         cv = {16, false, false,
               tab16 == 1 ? migrate_cluster2_kernel<16, false, false, false, TAB_F16, 4>
                          : migrate_cluster2_kernel<16, false, false, false, TAB_BF16, 4>,
               true};
-        vsel = kCluster2Default;
+        vsel = kCluster2Staged;
     }
-    const int pc2 = cv.nw * 32;
-    const size_t smem2 = cluster2_smem_bytes(M, pc2) + (cv.stage ? cluster2_stage_bytes(pc2) : 0) +
-                         (cv.ring ? cluster2_ring_bytes(pc2) : 0);
-    if (cluster_ok && !(flags & IMG2D_FLAG_CLUSTER_V1) && p->L >= 7 && smem2 + static_reserve <= (size_t)smem_optin) {
+    // Use variant v when its shared memory fits and, for windows wider than 8 CTAs, clusters of the
+    // needed size fit on the device.
+    auto try_cluster2 = [&](const Cluster2Variant &v, int index) {
+        const int pc2 = v.nw * 32;
+        const size_t smem2 = cluster2_smem_bytes(M, pc2) + (v.stage ? cluster2_stage_bytes(pc2) : 0) +
+                             (v.ring ? cluster2_ring_bytes(pc2) : 0);
+        if (smem2 + static_reserve > (size_t)smem_optin) return false;
         const int widest = make_groups(16);
         const int K = (widest + pc2 - 1) / pc2;
-        if (K <= 8 || (K <= kMaxCluster && clusters_that_fit((const void *)cv.fn, K, cv.nw * 32, smem2) > 0)) {
-            p->cluster = K;
-            p->G = 16;
-            p->fixed = true;
-            p->fn = cv.fn;
-            p->smem = smem2;
-            p->max_w = widest;
-            p->block = pc2;
-            p->variant = vsel;
-            p->kname = "migrate_cluster2";
-        }
+        if (!(K <= 8 || (K <= kMaxCluster && clusters_that_fit((const void *)v.fn, K, pc2, smem2) > 0))) return false;
+        p->cluster = K;
+        p->G = 16;
+        p->fixed = true;
+        p->fn = v.fn;
+        p->smem = smem2;
+        p->max_w = widest;
+        p->block = pc2;
+        p->variant = index;
+        p->kname = "migrate_cluster2";
+        return true;
+    };
+    if (cluster_ok && !(flags & IMG2D_FLAG_CLUSTER_V1) && p->L >= 7) {
+        // the default ring variant needs 33 KB more shared memory than the staged one: long
+        // operators or very wide windows fall back to the staged variant
+        if (!try_cluster2(cv, vsel) && !explicit_variant && !tab16 && vsel != kCluster2Staged)
+            try_cluster2(kCluster2[kCluster2Staged], kCluster2Staged);
     }
     if (tab16 && !p->cluster)
         return fail(IMG2D_EINVAL, "16-bit operator tables need the cluster kernel (>= 12 lane slots, 2M+1 >= 7, "

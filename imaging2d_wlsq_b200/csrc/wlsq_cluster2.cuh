@@ -108,11 +108,12 @@ __device__ __forceinline__ void cp_async4(void *smem_dst, const void *gsrc)
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
-// 16-byte global -> shared copy through L2 only (no L1 allocation)
-__device__ __forceinline__ void cp_async16(void *smem_dst, const void *gsrc)
+// 16-byte global -> shared copy through L2 only (no L1 allocation); `bytes` (0 or 16) are read
+// from global memory and the rest of the 16 are zero-filled
+__device__ __forceinline__ void cp_async16_zfill(void *smem_dst, const void *gsrc, unsigned bytes)
 {
     const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(gsrc) : "memory");
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(d), "l"(gsrc), "r"(bytes) : "memory");
 }
 // wait until at most N of this thread's most recent commit groups are still in flight
 template <int N>
@@ -264,10 +265,12 @@ __global__ void __launch_bounds__(NWARPS * 32, 1) migrate_cluster2_kernel(Migrat
         const char *row_q = tabb;
         unsigned nidx = 0;
         float cur_s = 0.f, cur_c = 0.f, nxt_s = 0.f, nxt_c = 0.f;
+        // branch-free: a pair outside the row becomes a zero-filled copy of nothing (never read)
         auto ring_copy = [&](int u) {
             const int pr = u + cq;
-            if (pr >= 0 && pr < npairs)
-                cp_async16(ringb + q * kRingSlots + (u & (kRingSlots - 1)), row_q + (size_t)pr * 16);
+            const bool ok = (unsigned)pr < (unsigned)npairs;
+            cp_async16_zfill(ringb + q * kRingSlots + (u & (kRingSlots - 1)), row_q + (ok ? pr : 0) * 16,
+                             ok ? 16u : 0u);
         };
         if (RING) {
             row_q = tabb + (size_t)idx_q[0] * row_bytes;
@@ -297,7 +300,7 @@ __global__ void __launch_bounds__(NWARPS * 32, 1) migrate_cluster2_kernel(Migrat
             } else if (RING) {
                 // this step's prologue pairs (copied at the end of the previous step) for the group
                 cp_async_wait_all();
-                __syncwarp(gmask);
+                __syncwarp();  // control flow is warp-uniform here
                 cur_s = nxt_s;
                 cur_c = nxt_c;
                 if (l + 1 < a.nextrap) {
@@ -371,7 +374,7 @@ __global__ void __launch_bounds__(NWARPS * 32, 1) migrate_cluster2_kernel(Migrat
                         ring_copy(u + 3);
                         cp_async_commit();
                         cp_async_wait<3>();
-                        __syncwarp(gmask);
+                        __syncwarp();  // control flow is warp-uniform here
                     }
                     {
                         const float4 va = sp[0];
@@ -467,7 +470,7 @@ __global__ void __launch_bounds__(NWARPS * 32, 1) migrate_cluster2_kernel(Migrat
                         case 2: cp_async_wait<1>(); break;
                         default: cp_async_wait<0>(); break;
                     }
-                    __syncwarp(gmask);
+                    __syncwarp();  // control flow is warp-uniform here
                 }
 #pragma unroll
                 for (int jj = 0; jj < X; ++jj) {
@@ -546,7 +549,7 @@ __global__ void __launch_bounds__(NWARPS * 32, 1) migrate_cluster2_kernel(Migrat
                 }
                 float img = ia + ib;
 #pragma unroll
-                for (int off = 1; off < Q; off <<= 1) img += __shfl_xor_sync(gmask, img, off);
+                for (int off = 1; off < Q; off <<= 1) img += __shfl_xor_sync(RING ? 0xffffffffu : gmask, img, off);
                 if (RING) {
                     if (jj == q) img_q = img;
                 } else if (prow && q == 0 && c0 + b * X + jj < W) {

@@ -263,37 +263,50 @@ def test_cluster2_variants_match_oracle(variant):
     _compact_check(w, img, wave, shot)
 
 
-def test_staged_default_matches_unstaged_bitwise():
-    """The default cluster kernel stages the next step's operator indices and Kahan partial rows in
-    shared memory (cp.async); its per-point arithmetic is that of variant 1, so the final
-    wavefields are bit-identical and the images agree to rounding of the partial split."""
+def test_staged_matches_unstaged_bitwise():
+    """Variant 11 stages the next step's operator indices and Kahan partial rows in shared memory
+    (cp.async); its per-point arithmetic is that of variant 1, so the final wavefields are
+    bit-identical and the images agree to rounding of the partial split."""
     w = synthetic.batched_uneven(nx=1500, nz=9, nf=4, ns=48, scale=1.0)
-    d0 = migration.Plan.for_workload(w).describe()
-    assert d0["kernel"] == "migrate_cluster2" and d0["variant"] == 10, d0
-    img0, _, wave0, shot0 = migration.migrate_workload(w)
+    img0, _, wave0, shot0 = migration.migrate_workload(w, variant=11)
     img1, _, wave1, shot1 = migration.migrate_workload(w, variant=1)
     assert np.array_equal(wave0, wave1) and np.array_equal(shot0, shot1)
     assert rel_l2(img0, img1) <= 1e-6
     _compact_check(w, img0, wave0, shot0)
 
 
-def test_ring_variant_matches_default_bitwise():
-    """Variant 12 reads the operator tap pairs from a per-lane-group shared-memory ring filled by
-    16-byte cp.async copies and keeps the next step's index and Kahan values in registers; the tap
-    values and the FMA order are those of the default, so final wavefields are bit-identical.  Runs
-    an operator length with a middle loop (35 taps) and the shortest one without (7 taps)."""
-    for taps in (35, 7):
-        w = synthetic.batched_uneven(nx=1500, nz=9, nf=4, ns=48, scale=1.0)
-        if taps != 2 * w.M + 1:
-            w.M = (taps - 1) // 2
-            w.table = operators.design_compact_table(w.nx, w.dx, w.dz, w.M, w.nk, w.dk)
-        d = migration.Plan.for_workload(w, variant=12).describe()
-        assert d["kernel"] == "migrate_cluster2" and d["variant"] == 11, d
+def _with_taps(w, taps):
+    if taps != 2 * w.M + 1:
+        w.M = (taps - 1) // 2
+        w.table = operators.design_compact_table(w.nx, w.dx, w.dz, w.M, w.nk, w.dk)
+    return w
+
+
+def test_ring_default_matches_staged_bitwise():
+    """The default (variant 12) reads the operator tap pairs from a per-lane-group shared-memory ring
+    filled by 16-byte cp.async copies and keeps the next step's index and Kahan values in registers;
+    the tap values and the FMA order are those of the staged variant 11, so final wavefields are
+    bit-identical.  Runs an operator length with a middle loop (35 taps), the shortest one without
+    (7 taps) and the longest whose ring still fits in shared memory (81 taps)."""
+    for taps in (35, 7, 81):
+        w = _with_taps(synthetic.batched_uneven(nx=1500, nz=9, nf=4, ns=48, scale=1.0), taps)
+        d = migration.Plan.for_workload(w).describe()
+        assert d["kernel"] == "migrate_cluster2" and d["variant"] == 11, (taps, d)
         img0, _, wave0, shot0 = migration.migrate_workload(w)
-        img1, _, wave1, shot1 = migration.migrate_workload(w, variant=12)
+        img1, _, wave1, shot1 = migration.migrate_workload(w, variant=11)
         assert np.array_equal(wave0, wave1) and np.array_equal(shot0, shot1), taps
         assert rel_l2(img0, img1) <= 1e-6, taps
-        _compact_check(w, img1, wave1, shot1)
+        _compact_check(w, img0, wave0, shot0)
+
+
+def test_long_operator_falls_back_to_staged_variant():
+    """91 taps leave no room for the 33 KB ring next to the wavefields and halos: the default plan
+    takes the staged variant, still on the cluster kernel."""
+    w = _with_taps(synthetic.batched_uneven(nx=1500, nz=5, nf=3, ns=48, scale=1.0), 91)
+    d = migration.Plan.for_workload(w).describe()
+    assert d["kernel"] == "migrate_cluster2" and d["variant"] == 10, d
+    img, _, wave, shot = migration.migrate_workload(w)
+    _compact_check(w, img, wave, shot)
 
 
 def test_wide_window_non_portable_cluster():
