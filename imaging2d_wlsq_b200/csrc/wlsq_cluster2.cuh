@@ -486,10 +486,13 @@ __global__ void __launch_bounds__(NWARPS * 32, 1) migrate_cluster2_kernel(Migrat
                     }
                 }
             }
+            // outputs outside every shot aperture of their slot stay zero; most lanes have none
+            if ((in_a & in_b) != (1u << X) - 1u) {
 #pragma unroll
-            for (int jj = 0; jj < X; ++jj) {
-                if (!((in_a >> jj) & 1u)) acc[jj][0] = acc[jj][1] = acc[jj][2] = acc[jj][3] = 0.f;
-                if (!((in_b >> jj) & 1u)) acc[jj][4] = acc[jj][5] = acc[jj][6] = acc[jj][7] = 0.f;
+                for (int jj = 0; jj < X; ++jj) {
+                    if (!((in_a >> jj) & 1u)) acc[jj][0] = acc[jj][1] = acc[jj][2] = acc[jj][3] = 0.f;
+                    if (!((in_b >> jj) & 1u)) acc[jj][4] = acc[jj][5] = acc[jj][6] = acc[jj][7] = 0.f;
+                }
             }
             if (RING) {
                 // every ring slot has been read: copy the next step's prologue pairs (u < 0) now, so
