@@ -6,8 +6,10 @@
 //   * the tap loop is a compact runtime loop over tap pairs with a short static prologue and
 //     epilogue, which keeps the loop body in the instruction cache and serves every odd operator
 //     length L >= 7 with one instance;
-//   * the Kahan partial-image rows of the next depth step are prefetched into L1 while the
-//     current step computes, so the imaging read-modify-write does not wait on DRAM.
+//   * in the default form (OPT bit 3) the operator tap pairs reach the tap loop through a small
+//     per-lane-group shared-memory ring filled by cp.async a few tap pairs ahead, and the next
+//     depth step's operator index and Kahan partial-image values are loaded into registers one step
+//     ahead, so neither the tap loop nor the imaging read-modify-write waits on L2 or DRAM.
 //
 // Tap loop (input-stationary): input position t (0 <= t < X+L-1, relative to block start - M)
 // contributes to output jj with tap k = t - jj when 0 <= k < L.  Taps are loaded in pairs (k, k+1)
