@@ -12,6 +12,7 @@
 #pragma once
 #include "wlsq_adjoint.cuh"
 #include "wlsq_cluster.cuh"
+#include "wlsq_cluster2.cuh"
 
 namespace img2d {
 
@@ -80,6 +81,67 @@ __device__ __forceinline__ void fir2_forward(const DemigrateArgs &a, const float
     }
 }
 
+// The forward step with the operator pairs read from the lane group's shared-memory ring (the
+// migration kernel's scheme): lane q copies the pairs of output q's row with 16-byte cp.async through
+// L2, three tap-loop iterations before they are read.  Output jj reads pair p at iteration
+// u = p - (X - jj) / 2 from slot u mod 4; iteration u's reads happen at steps t = 2u+7 (odd jj) and
+// 2u+8 (even jj).  The pairs with u < 0 are copied on entry, u = 0, 1, 2 after steps 0, 2, 4, and
+// u + 3 at the start of iteration u, one commit group each.  Same taps, same FMA order as
+// fir2_forward.
+template <int X, int L>
+__device__ __forceinline__ void fir2_forward_ring(const DemigrateArgs &a, const float4 *src, const uint16_t *sidx,
+                                                 int xm0, int pb, int q, float4 *ring, float (&acc)[X][4])
+{
+    static_assert(L > 0 && X == 8 && kDcQ == X, "lane q owns output q of the block");
+    constexpr int M = (L - 1) / 2, NP = (L + 1) / 2;
+    const int hstride = a.tab_stride >> 1;
+    const float4 *rowq = reinterpret_cast<const float4 *>(a.tab) + (long long)sidx[min(xm0 + q, a.nx - 1)] * hstride;
+    const int cq = (X - q) >> 1;
+    auto copy = [&](int u) {
+        const int pr = u + cq;
+        const bool ok = (unsigned)pr < (unsigned)NP;
+        cp_async16_zfill(ring + q * kRingSlots + (u & (kRingSlots - 1)), rowq + (ok ? pr : 0), ok ? 16u : 0u);
+    };
+#pragma unroll
+    for (int u = -(X / 2); u < 0; ++u) copy(u);
+    cp_async_commit();
+    cp_async_wait<0>();
+    __syncwarp();
+#pragma unroll
+    for (int jj = 0; jj < X; ++jj) acc[jj][0] = acc[jj][1] = acc[jj][2] = acc[jj][3] = 0.f;
+    float4 tf[X];
+#pragma unroll
+    for (int t = 0; t < X + L - 1; ++t) {
+        if (t >= X - 1 && ((t - (X - 1)) & 1) == 0) {
+            // start of iteration u: copy iteration u + 3, wait for iteration u
+            const int u = (t - (X - 1)) >> 1;
+            if (u + 3 <= NP - 1) {
+                copy(u + 3);
+                cp_async_commit();
+            }
+            const int newer = (u + 3 < NP - 1 ? u + 3 : NP - 1) - u;
+            if (newer >= 3) cp_async_wait<3>();
+            else if (newer == 2) cp_async_wait<2>();
+            else if (newer == 1) cp_async_wait<1>();
+            else cp_async_wait<0>();
+            __syncwarp();
+        }
+        const float4 v = src[(pb - M + t) * kDcQ];
+#pragma unroll
+        for (int jj = 0; jj < X; ++jj) {
+            const int k = t - jj;
+            if (k >= 0 && k < L) {
+                if ((k & 1) == 0) tf[jj] = ring[jj * kRingSlots + (((k >> 1) - ((X - jj) >> 1)) & (kRingSlots - 1))];
+                mac2(acc[jj], (k & 1) ? tf[jj].z : tf[jj].x, (k & 1) ? tf[jj].w : tf[jj].y, v);
+            }
+        }
+        if (t < 6 && (t & 1) == 0 && (t >> 1) <= NP - 1) {
+            copy(t >> 1);
+            cp_async_commit();
+        }
+    }
+}
+
 // Transposed step of a block of X outputs: output y takes tap y+M-i of the row of input i.
 template <int X, int L>
 __device__ __forceinline__ void fir2_transposed(const DemigrateArgs &a, const float4 *src, const uint16_t *sidx,
@@ -124,11 +186,23 @@ __device__ __forceinline__ void fir2_transposed(const DemigrateArgs &a, const fl
     }
 }
 
+// Shared memory of the forward step's tap-pair ring (RING): per lane group X rows x kRingSlots
+// pairs plus one 16-byte pad, after the index rows rounded up to 16 bytes.
+__host__ __device__ inline size_t demigc_ring_offset(int M) { return (demigc_smem_bytes(M) + 15) / 16 * 16; }
+__host__ __device__ inline size_t demigc_ring_smem_bytes(int M)
+{
+    return demigc_ring_offset(M) + (size_t)(kDcPC / kDcX) * (kDcX * kRingSlots + 1) * 16;
+}
+
 // L > 0: compile-time operator length; L == 0: runtime length a.M.  work / ckpt_items hold float4
 // planes of PC x 8 lanes per CTA: per CTA ckpt[nslab], slab[D], save; the cache [item][rank][nslab].
-template <int L>
+// RING (L > 0): the forward steps read their operator pairs through the lane group's shared-memory
+// ring (fir2_forward_ring), and the next step's index row is loaded into registers at the start of
+// a step and stored to shared memory at its end, so the ring's cp.async groups are the only ones.
+template <int L, bool RING = false>
 __global__ void __launch_bounds__(kDcNW * 32, 1) demigrate_cluster_kernel(DemigrateArgs a)
 {
+    static_assert(!RING || L > 0, "the ring needs a compile-time operator length");
     constexpr int Q = kDcQ, P = kDcP, X = kDcX, PC = kDcPC;
     const int M = L > 0 ? (L - 1) / 2 : a.M;
     const int MP = demigc_mp(M);
@@ -145,6 +219,8 @@ __global__ void __launch_bounds__(kDcNW * 32, 1) demigrate_cluster_kernel(Demigr
     const int b = warp * P + p;  // this lane group's block: local positions [b*X, b*X+X)
     const int c0 = (int)crank * PC;
     const bool has_left = crank > 0, has_right = crank + 1 < csize;
+    float4 *const ring = reinterpret_cast<float4 *>(reinterpret_cast<char *>(sm4) + demigc_ring_offset(M)) +
+                         (size_t)b * (X * kRingSlots + 1);
     const unsigned rank0_item = map_rank(&s_item, 0);
     const long long pe = (long long)PC * Q;  // float4 per plane
     float4 *work = reinterpret_cast<float4 *>(a.work) + (long long)blockIdx.x * (a.work_cta / 2);
@@ -217,11 +293,31 @@ __global__ void __launch_bounds__(kDcNW * 32, 1) demigrate_cluster_kernel(Demigr
         const int pb = MP + b * X;      // its buffer position
         unsigned *cur = sidx0, *nxt = sidx1;
         auto step_idx = [&]() { return reinterpret_cast<const uint16_t *>(cur) - ibase; };
+        // RING: this thread's word of the next step's index row (at most one: the row has fewer
+        // words than the CTA has threads), loaded at the start of a step, stored at its end
+        unsigned iw = 0;
+        int iw_k = -1;
         auto stage_next = [&](int nl) {
-            if (nl >= 0) demig_stage_idx(a, idx_j, nl, base, PC, MP, nxt);
+            if (RING) {
+                iw_k = -1;
+                if (nl >= 0) {
+                    const int lo = max(0, base - MP) >> 1, hi = (min(a.nx, base + PC + MP) + 1) >> 1;
+                    const int k = lo + (int)threadIdx.x;
+                    if (k < hi) {
+                        iw = reinterpret_cast<const unsigned *>(idx_j + (long long)nl * a.idx_lstride)[k];
+                        iw_k = k - lo;
+                    }
+                }
+            } else if (nl >= 0) {
+                demig_stage_idx(a, idx_j, nl, base, PC, MP, nxt);
+            }
         };
         auto end_step = [&]() {
-            asm volatile("cp.async.wait_group 0;" ::: "memory");
+            if (RING) {
+                if (iw_k >= 0) nxt[iw_k] = iw;
+            } else {
+                asm volatile("cp.async.wait_group 0;" ::: "memory");
+            }
             cluster_arrive();
             cluster_wait();
             unsigned *t = cur; cur = nxt; nxt = t;
@@ -255,7 +351,8 @@ __global__ void __launch_bounds__(kDcNW * 32, 1) demigrate_cluster_kernel(Demigr
         auto forward_step = [&](int l, float4 *keep, int nl) {
             stage_next(nl);
             float acc[X][4];
-            fir2_forward<X, L>(a, bufA + q, step_idx(), xm0, pb, M, acc);
+            if constexpr (RING) fir2_forward_ring<X, L>(a, bufA + q, step_idx(), xm0, pb, q, ring, acc);
+            else fir2_forward<X, L>(a, bufA + q, step_idx(), xm0, pb, M, acc);
 #pragma unroll
             for (int jj = 0; jj < X; ++jj) {
                 mask(acc[jj], jj);

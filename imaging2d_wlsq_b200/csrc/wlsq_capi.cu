@@ -141,20 +141,24 @@ static const DemigKernel kDemig[] = {IMG2D_DEMIG_G(2), IMG2D_DEMIG_G(4), IMG2D_D
 struct DemigClusterKernel {
     int L;
     DemigFn fn;
+    DemigFn ring;  // forward steps through the shared-memory tap-pair ring (compile-time L only)
 };
 static const DemigClusterKernel kDemigCluster[] = {
-    {0, demigrate_cluster_kernel<0>},   {25, demigrate_cluster_kernel<25>}, {31, demigrate_cluster_kernel<31>},
-    {35, demigrate_cluster_kernel<35>}, {55, demigrate_cluster_kernel<55>},
+    {0, demigrate_cluster_kernel<0>, nullptr},
+    {25, demigrate_cluster_kernel<25>, demigrate_cluster_kernel<25, true>},
+    {31, demigrate_cluster_kernel<31>, demigrate_cluster_kernel<31, true>},
+    {35, demigrate_cluster_kernel<35>, demigrate_cluster_kernel<35, true>},
+    {55, demigrate_cluster_kernel<55>, demigrate_cluster_kernel<55, true>},
 };
 
-static DemigFn find_demig_cluster(int L)
+static DemigFn find_demig_cluster(int L, bool ring = false)
 {
     DemigFn generic = nullptr;
     for (const auto &k : kDemigCluster) {
-        if (k.L == L) return k.fn;
+        if (k.L == L) return ring ? k.ring : k.fn;
         if (k.L == 0) generic = k.fn;
     }
-    return generic;
+    return ring ? nullptr : generic;
 }
 
 static DemigFn find_demig(int G, int L)
@@ -363,6 +367,7 @@ struct img2d_plan {
     // demigration (adjoint) launch state, built on its first call
     int adj_G = 0, adj_grid = 0, adj_items_n = 0, adj_wmax = 0, adj_block = 0, adj_slab = 0, adj_nslab = 0;
     int adj_cluster = 0;               // CTAs per cluster of the cluster demigration kernel, 0 = single CTA
+    bool adj_ring = false;             // its forward steps read operator pairs through the shared-memory ring
     long long adj_work_cta = 0, adj_cache_item = 0;  // float2 elements: per-CTA work area, kept per item
     size_t adj_smem = 0;
     void (*adj_fn)(img2d::DemigrateArgs) = nullptr;
@@ -831,22 +836,28 @@ static int demig_prepare(img2d_plan *p, int slab)
     std::vector<int4> segs;
     std::vector<int16_t> owner;
     int G = 8, widest = 0, K = 0;
+    bool ring = false;
     DemigFn fn = nullptr;
     size_t smem = 0;
     // Cluster kernel (16 slots per item, 512 positions per CTA) when there are enough slots to fill
-    // it and the widest window fits 8 CTAs; otherwise the single-CTA kernel.
-    if (p->n_slots >= 12 && !(p->flags & IMG2D_FLAG_NO_CLUSTER) &&
-        demigc_smem_bytes(p->M) + static_reserve <= (size_t)smem_optin) {
+    // it and the widest window fits 16 CTAs, with the forward steps' tap-pair ring where the operator
+    // length has an instance and its shared memory fits; otherwise the single-CTA kernel.
+    if (p->n_slots >= 12 && !(p->flags & IMG2D_FLAG_NO_CLUSTER)) {
         widest = pack_groups(p, 16, groups, segs, owner);
         const int k = (widest + kDcPC - 1) / kDcPC;
-        DemigFn cfn = find_demig_cluster(p->L);
-        if (k <= 8 || (k <= kMaxCluster && cfn &&
-                       clusters_that_fit((const void *)cfn, k, kDcNW * 32, demigc_smem_bytes(p->M)) > 0)) {
-            K = k;
-            G = 16;
-            fn = find_demig_cluster(p->L);
-            smem = demigc_smem_bytes(p->M);
-        }
+        auto try_fn = [&](DemigFn cfn, size_t csmem, bool is_ring) {
+            if (!cfn || K || csmem + static_reserve > (size_t)smem_optin) return;
+            if (k <= 8 || (k <= kMaxCluster && clusters_that_fit((const void *)cfn, k, kDcNW * 32, csmem) > 0)) {
+                K = k;
+                G = 16;
+                fn = cfn;
+                smem = csmem;
+                ring = is_ring;
+            }
+        };
+        if (!(p->flags & IMG2D_FLAG_DEMIG_NO_RING))
+            try_fn(find_demig_cluster(p->L, true), demigc_ring_smem_bytes(p->M), true);
+        try_fn(find_demig_cluster(p->L), demigc_smem_bytes(p->M), false);
     }
     if (!K) {
         for (;; G >>= 1) {
@@ -921,6 +932,7 @@ static int demig_prepare(img2d_plan *p, int slab)
     p->adj_nslab = nslab;
     p->adj_smem = smem;
     p->adj_fn = fn;
+    p->adj_ring = ring;
     return IMG2D_OK;
 }
 
@@ -1201,10 +1213,10 @@ int img2d_plan_describe_demigration(const img2d_plan *p, char *buf, int buflen)
     snprintf(buf, buflen,
              "{\"kernel\": \"%s\", \"cluster\": %d, \"G\": %d, \"X\": 8, \"L\": %d, \"grid\": %d, \"block\": %d, "
              "\"smem\": %zu, \"items\": %d, \"max_union_width\": %d, \"slab\": %d, \"slabs\": %d, "
-             "\"workspace_bytes\": %zu, \"source_cache_bytes\": %zu}",
+             "\"workspace_bytes\": %zu, \"source_cache_bytes\": %zu, \"ring\": %s}",
              p->adj_cluster ? "demigrate_cluster" : "demigrate", p->adj_cluster, p->adj_G, p->L, p->adj_grid,
              p->adj_block, p->adj_smem, p->adj_items_n, p->adj_wmax, p->adj_slab,
-             p->adj_nslab, p->adj_work.bytes, p->adj_cache.bytes);
+             p->adj_nslab, p->adj_work.bytes, p->adj_cache.bytes, p->adj_ring ? "true" : "false");
     return IMG2D_OK;
 }
 

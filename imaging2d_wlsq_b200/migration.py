@@ -70,9 +70,10 @@ class Plan:
     """Device-resident migration plan (torch CUDA tensors in, torch CUDA tensors out)."""
 
     def __init__(self, ns, nextrap, nz, nx, nf, nt, M, nk, shot_x0=None, shot_nx=None, two_tables=False,
-                 generic=False, no_cluster=False, cluster_v1=False, variant=0, table="fp32"):
+                 generic=False, no_cluster=False, cluster_v1=False, variant=0, table="fp32", demig_ring=True):
         """table: operator-table storage, "fp32" (default), "fp16" or "bf16" (reduced-precision
-        storage, FP32 arithmetic; cluster kernel only)."""
+        storage, FP32 arithmetic; cluster kernel only).  demig_ring: the cluster demigration kernel's
+        forward steps read their operator pairs through a shared-memory ring (False: through L1)."""
         self.ns, self.nextrap, self.nz, self.nx, self.nf, self.nt, self.M, self.nk = \
             ns, nextrap, nz, nx, nf, nt, M, nk
         x0 = None if shot_x0 is None else np.ascontiguousarray(shot_x0, dtype=np.int32)
@@ -80,7 +81,8 @@ class Plan:
         flags = (_lib.FLAG_TWO_TABLES if two_tables else 0) | (_lib.FLAG_GENERIC if generic else 0) | \
             (_lib.FLAG_NO_CLUSTER if no_cluster else 0) | (_lib.FLAG_CLUSTER_V1 if cluster_v1 else 0) | \
             (int(variant) << _lib.FLAG_VARIANT_SHIFT) | \
-            {"fp32": 0, "fp16": _lib.FLAG_TABLE_FP16, "bf16": _lib.FLAG_TABLE_BF16}[table]
+            {"fp32": 0, "fp16": _lib.FLAG_TABLE_FP16, "bf16": _lib.FLAG_TABLE_BF16}[table] | \
+            (0 if demig_ring else _lib.FLAG_DEMIG_NO_RING)
         h = ctypes.c_void_p()
         check(lib().img2d_plan_create(ctypes.byref(h), ns, nextrap, nz, nx, nf, nt, M, nk, ptr(x0), ptr(wn), flags))
         self._h = h

@@ -210,6 +210,7 @@ def test_cluster_demigration_matches_oracle_and_single_cta(case, slab):
         data[mode] = d.cpu().numpy()
     desc = op.plan.describe_demigration()
     assert desc["kernel"] == "demigrate_cluster" and desc["G"] == 16, desc
+    assert desc["ring"] == (2 * w.M + 1 in (25, 31, 35, 55)), desc  # compile-time lengths
     if w.nx > 512:
         assert desc["cluster"] >= 2, desc
     single = lsm.MigrationOperator.for_workload(w, slab_depth=slab, no_cluster=True)
@@ -225,6 +226,21 @@ def test_cluster_demigration_matches_oracle_and_single_cta(case, slab):
     assert rel_norms <= 1e-6 and rel <= 2e-5, (lhs, rhs, rel, rel_norms)
     op.plan.close()
     single.plan.close()
+
+
+def test_demigration_ring_matches_l1_path_bitwise():
+    """The cluster demigration's forward steps read their operator pairs through a shared-memory ring
+    (cp.async) by default; the same kernel reading them through L1 gives bit-identical data."""
+    import torch
+    w = synthetic.batched_uneven(nx=1300, nz=9, nf=3, ns=64)
+    m = torch.from_numpy(np.random.default_rng(5).standard_normal((w.nextrap, w.nx)).astype(np.float32)).cuda()
+    out = {}
+    for ring in (True, False):
+        op = lsm.MigrationOperator.for_workload(w, slab_depth=3, demig_ring=ring)
+        out[ring] = op.demigrate(m).cpu().numpy()
+        assert op.plan.describe_demigration()["ring"] == ring
+        op.plan.close()
+    assert np.array_equal(out[True], out[False])
 
 
 def test_wide_window_non_portable_cluster_demigration():
