@@ -194,61 +194,6 @@ __host__ __device__ inline size_t demigc_ring_smem_bytes(int M)
     return demigc_ring_offset(M) + (size_t)(kDcPC / kDcX) * (kDcX * kRingSlots + 1) * 16;
 }
 
-// The transposed step with the operator pairs read from the lane group's shared-memory ring.  Step t
-// of the input-stationary loop reads taps k = jj + 2M - t (jj = 0 .. X-1, 0 <= k < L) of the row of
-// input position t, at most five 16-byte pairs, starting at pair plo(t) = max(0, 2M - t) / 2.
-// Lane q < 5 copies pair plo(t) + q of that row into slot t mod 4 of the ring (five entries per
-// slot; lanes 5-7 write zeros to three spare entries), three steps before step t reads it, one
-// commit group per step.  Same taps, same FMA order as fir2_transposed.
-template <int X, int L>
-__device__ __forceinline__ void fir2_transposed_ring(const DemigrateArgs &a, const float4 *src, const uint16_t *sidx,
-                                                    int xm0, int pb, int q, float4 *ring, float (&acc)[X][4])
-{
-    static_assert(L > 0 && X == 8 && kDcQ == X, "lane group of 8 per block of 8 outputs");
-    static_assert(4 * 5 + 3 <= X * kRingSlots + 1, "the transposed ring fits in the forward ring's area");
-    constexpr int M = (L - 1) / 2, T = X + L - 1;
-    const int hstride = a.tab_stride >> 1;
-    const float4 *tab4 = reinterpret_cast<const float4 *>(a.tab);
-    auto copy = [&](int t) {
-        const int klo = 2 * M - t > 0 ? 2 * M - t : 0;
-        const int khi = X - 1 + 2 * M - t < L - 1 ? X - 1 + 2 * M - t : L - 1;
-        const int plo = klo >> 1, n = (khi >> 1) - plo + 1;
-        int xm = xm0 - M + t;
-        xm = xm < 0 ? 0 : (xm < a.nx ? xm : a.nx - 1);
-        const float4 *rp = tab4 + (long long)sidx[xm] * hstride;
-        const bool ok = q < n;
-        cp_async16_zfill(ring + (q < 5 ? (t & 3) * 5 + q : 15 + q), rp + (ok ? plo + q : 0), ok ? 16u : 0u);
-        cp_async_commit();
-    };
-    copy(0);
-    copy(1);
-    copy(2);
-#pragma unroll
-    for (int jj = 0; jj < X; ++jj) acc[jj][0] = acc[jj][1] = acc[jj][2] = acc[jj][3] = 0.f;
-#pragma unroll
-    for (int t = 0; t < T; ++t) {
-        if (t + 3 < T) copy(t + 3);
-        const int newer = (t + 3 < T - 1 ? t + 3 : T - 1) - t;
-        if (newer >= 3) cp_async_wait<3>();
-        else if (newer == 2) cp_async_wait<2>();
-        else if (newer == 1) cp_async_wait<1>();
-        else cp_async_wait<0>();
-        __syncwarp();
-        const float4 v = src[(pb - M + t) * kDcQ];
-        const int plo = (2 * M - t > 0 ? 2 * M - t : 0) >> 1;
-        float4 cur = make_float4(0.f, 0.f, 0.f, 0.f);
-        const int jj0 = t - 2 * M > 0 ? t - 2 * M : 0;
-#pragma unroll
-        for (int jj = 0; jj < X; ++jj) {
-            const int k = jj + 2 * M - t;
-            if (k >= 0 && k < L) {
-                if ((k & 1) == 0 || jj == jj0) cur = ring[(t & 3) * 5 + (k >> 1) - plo];
-                mac2(acc[jj], (k & 1) ? cur.z : cur.x, (k & 1) ? cur.w : cur.y, v);
-            }
-        }
-    }
-}
-
 // L > 0: compile-time operator length; L == 0: runtime length a.M.  work / ckpt_items hold float4
 // planes of PC x 8 lanes per CTA: per CTA ckpt[nslab], slab[D], save; the cache [item][rank][nslab].
 // RING (L > 0): the forward steps read their operator pairs through the lane group's shared-memory
@@ -467,8 +412,7 @@ __global__ void __launch_bounds__(kDcNW * 32, 1) demigrate_cluster_kernel(Demigr
                 const float4 *Sl = (l > lb) ? slabbuf + (long long)(l - 1 - lb) * pe : ckpt + (long long)c * pe;
                 const float *mrow = l > 0 ? a.refl + (long long)(l - 1) * a.nx + base : nullptr;
                 float acc[X][4];
-                if constexpr (RING) fir2_transposed_ring<X, L>(a, bufA + q, step_idx(), xm0, pb, q, ring, acc);
-                else fir2_transposed<X, L>(a, bufA + q, step_idx(), xm0, pb, M, acc);
+                fir2_transposed<X, L>(a, bufA + q, step_idx(), xm0, pb, M, acc);
 #pragma unroll
                 for (int jj = 0; jj < X; ++jj) {
                     mask(acc[jj], jj);
