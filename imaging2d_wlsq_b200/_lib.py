@@ -80,6 +80,8 @@ def load():
     lib.img2d_plan_execute.argtypes = [c_void_p] * 6
     lib.img2d_plan_execute_naive.restype = c_int
     lib.img2d_plan_execute_naive.argtypes = [c_void_p] * 5
+    lib.img2d_plan_dense_table.restype = c_int
+    lib.img2d_plan_dense_table.argtypes = [c_void_p, c_int, c_void_p, c_void_p]
     lib.img2d_plan_shot_offset.restype = c_longlong
     lib.img2d_plan_shot_offset.argtypes = [c_void_p, c_int]
     lib.img2d_plan_wavefield_elems.restype = c_longlong

@@ -235,6 +235,33 @@ __global__ void naive_unpack_kernel(const float4 *__restrict__ buf, int w, int M
     shot[i] = cpx{v.z, -v.w};
 }
 
+// Dense operator table of the reference's legacy ABI from the compact table and the operator index:
+// dense[l][j][x][k] = tab[idx[j][l][x]][k] (conjugated when conj != 0).  One block per (l, j) row of
+// nx*L elements, written with coalesced stores; x and k advance incrementally with the block stride.
+__global__ void dense_table_kernel(const uint16_t *__restrict__ idx, int nf, int nextrap, int nx, int lstride,
+                                   const cpx *__restrict__ tab, int tab_stride, int L, int conj,
+                                   cpx *__restrict__ dense)
+{
+    const int lj = blockIdx.x;  // l * nf + j
+    const int l = lj / nf, j = lj - l * nf;
+    const uint16_t *irow = idx + ((long long)j * nextrap + l) * lstride;
+    cpx *out = dense + (long long)lj * nx * L;
+    const int n = nx * L;
+    const int sx = (int)blockDim.x / L, sk = (int)blockDim.x - sx * L;
+    int x = (int)threadIdx.x / L, k = (int)threadIdx.x - x * L;
+    for (int e = threadIdx.x; e < n; e += blockDim.x) {
+        cpx v = tab[(long long)irow[x] * tab_stride + k];
+        if (conj) v.im = -v.im;
+        out[e] = v;
+        x += sx;
+        k += sk;
+        if (k >= L) {
+            k -= L;
+            ++x;
+        }
+    }
+}
+
 // L2 read probe: every thread streams float4 from an L2-resident buffer with ld.global.cg (L2 only,
 // no L1 allocation); four independent accumulators keep many loads in flight.
 __global__ void l2_read_probe_kernel(const float4 *__restrict__ buf, long long n4, int iters, float *out)
@@ -368,6 +395,7 @@ struct img2d_plan {
     int adj_G = 0, adj_grid = 0, adj_items_n = 0, adj_wmax = 0, adj_block = 0, adj_slab = 0, adj_nslab = 0;
     int adj_cluster = 0;               // CTAs per cluster of the cluster demigration kernel, 0 = single CTA
     bool adj_ring = false;             // its forward steps read operator pairs through the shared-memory ring
+    bool model_set = false;            // set_model has built the padded tables and the operator index
     long long adj_work_cta = 0, adj_cache_item = 0;  // float2 elements: per-CTA work area, kept per item
     size_t adj_smem = 0;
     void (*adj_fn)(img2d::DemigrateArgs) = nullptr;
@@ -815,6 +843,7 @@ static int set_model(img2d_plan *p, const double *d_omega, const double *d_vel, 
     index_table_kernel<<<blocks, 256, 0, st>>>(d_omega, d_vel, p->nf, p->nextrap, p->nx, p->idx_lstride, p->nk,
                                                dk, p->idx.as<uint16_t>());
     IMG2D_CUDA(cudaGetLastError());
+    p->model_set = true;
     return IMG2D_OK;
 }
 
@@ -1217,6 +1246,26 @@ int img2d_plan_describe_demigration(const img2d_plan *p, char *buf, int buflen)
              p->adj_cluster ? "demigrate_cluster" : "demigrate", p->adj_cluster, p->adj_G, p->L, p->adj_grid,
              p->adj_block, p->adj_smem, p->adj_items_n, p->adj_wmax, p->adj_slab,
              p->adj_nslab, p->adj_work.bytes, p->adj_cache.bytes, p->adj_ring ? "true" : "false");
+    return IMG2D_OK;
+}
+
+int img2d_plan_dense_table(const img2d_plan *p, int which, img2d_c64 *d_dense, void *stream)
+{
+    if (!p) return fail(IMG2D_EINVAL, "plan is NULL");
+    if (!d_dense) return fail(IMG2D_EINVAL, "d_dense is NULL");
+    if (which != 0 && which != 1) return fail(IMG2D_EINVAL, "which must be 0 (forward) or 1 (receiver)");
+    if (p->mode == OP_DENSE) return fail(IMG2D_EINVAL, "a dense-table plan has no compact table");
+    if (!p->model_set) return fail(IMG2D_EINVAL, "call img2d_plan_set_model first");
+    if ((long long)p->nx * p->L >= (1ll << 31) || (long long)p->nextrap * p->nf >= (1ll << 31))
+        return fail(IMG2D_EINVAL, "dense table rows too large");
+    const bool back_rows = which == 1 && p->mode == OP_TWO;
+    const cpx *tab = back_rows ? p->tabB.as<cpx>() : p->tabF.as<cpx>();
+    const int conj = which == 1 && !back_rows;
+    cudaStream_t st = (cudaStream_t)stream;
+    dense_table_kernel<<<p->nextrap * p->nf, 256, 0, st>>>(p->idx.as<uint16_t>(), p->nf, p->nextrap, p->nx,
+                                                          p->idx_lstride, tab, p->tab_stride, p->L, conj,
+                                                          (cpx *)d_dense);
+    IMG2D_CUDA(cudaGetLastError());
     return IMG2D_OK;
 }
 

@@ -134,6 +134,19 @@ class Plan:
         check(lib().img2d_plan_describe_demigration(self._h, buf, 512))
         return json.loads(buf.value.decode())
 
+    def dense_table(self, which=0, out=None, stream=None):
+        """The legacy ABI's dense operator table (nextrap, nf, nx, 2M+1) complex64, gathered on the
+        device from the compact table and the operator index set by set_model (the GPU form of
+        makeTableOfOperators, preparation.py:101-115).  which=0: forward rows; 1: receiver rows."""
+        import torch
+        shape = (self.nextrap, self.nf, self.nx, 2 * self.M + 1)
+        if out is None:
+            out = torch.empty(shape, dtype=torch.complex64, device="cuda")
+        if tuple(out.shape) != shape or out.dtype != torch.complex64 or not out.is_contiguous():
+            raise ValueError("out must be a contiguous complex64 tensor of shape %s" % (shape,))
+        check(lib().img2d_plan_dense_table(self._h, int(which), ptr(out), self._stream(stream)))
+        return out
+
     def execute_naive(self, wave, shot, image, stream=None):
         check(lib().img2d_plan_execute_naive(self._h, ptr(wave), ptr(shot), ptr(image), self._stream(stream)))
 

@@ -114,6 +114,13 @@ int img2d_plan_execute(img2d_plan *plan, img2d_c64 *d_wave, img2d_c64 *d_shot, f
                        float *d_image_shots, void *stream);
 /* Element offset of shot s's block inside the packed wavefield arrays, and their total size. */
 long long img2d_plan_shot_offset(const img2d_plan *plan, int s);
+/* Dense operator table of the reference's legacy ABI, (nextrap, nf, nx, 2M+1) complex64 written to
+ * d_dense on the device from the plan's compact table and operator index (after set_model):
+ * entry [l][j][x] is the table row of find_nearest(kappa, w[j]/v[l,x]).  which = 0: forward rows;
+ * 1: receiver rows (tab_back in two-table plans, else the conjugated forward rows).  Replaces the
+ * host-side gather of py_src/operatorsPreparation/preparation.py:101-115 (makeTableOfOperators)
+ * for callers that keep passing dense tables to `extrapolate`.  Asynchronous on `stream`. */
+int img2d_plan_dense_table(const img2d_plan *plan, int which, img2d_c64 *d_dense, void *stream);
 long long img2d_plan_wavefield_elems(const img2d_plan *plan);
 /* Device bytes held by the plan, and the kernel configuration it chose. */
 size_t img2d_plan_workspace_bytes(const img2d_plan *plan);
