@@ -398,6 +398,49 @@ def frontend_leg(dev, w):
     }
 
 
+def dense_table_leg(dev, nl=100, cpu_nl=2):
+    """The legacy ABI's dense operator table built on the device (img2d_plan_dense_table) for the
+    plain medium geometry (nx=1024, nf=256 over 2-40 Hz, 31 taps, nk=2000): the first `nl` depth steps
+    (6.5 GB of complex64, written once).  CPU: the numpy gather of operators.dense_table (the
+    vectorised form of preparation.py:101-115) on the first `cpu_nl` depth steps, one host core; its
+    rows are compared bit for bit with the device's."""
+    import time as _time
+    import torch
+    from imaging2d_wlsq_b200 import migration, operators, synthetic
+    w = synthetic.plain_medium()
+    L = 2 * w.M + 1
+    plan = migration.Plan(w.ns, nl, w.nz, w.nx, w.nf, w.nt, w.M, w.nk)
+    plan.set_model(torch.from_numpy(w.omega).to(dev), torch.from_numpy(np.ascontiguousarray(w.velocity)).to(dev),
+                   w.dk, torch.from_numpy(w.table).to(dev))
+    out = torch.empty((nl, w.nf, w.nx, L), dtype=torch.complex64, device=dev)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    plan.dense_table(0, out=out)
+    best = 1e30
+    for _ in range(3):
+        e0.record()
+        plan.dense_table(0, out=out)
+        e1.record()
+        e1.synchronize()
+        best = min(best, e0.elapsed_time(e1) / 1e3)
+    head = out[:cpu_nl].cpu().numpy()
+    plan.close()
+    nbytes = out.numel() * 8
+    del out
+    torch.cuda.empty_cache()
+    c0 = _time.perf_counter()
+    host = operators.dense_table(w.table, w.omega, w.velocity, cpu_nl, dk=w.dk)
+    c_s = _time.perf_counter() - c0
+    rows = nl * w.nf * w.nx
+    return {"workload": f"plain_medium geometry: first {nl} of {w.nz} depth steps, nf={w.nf} nx={w.nx} "
+                        f"taps={L} nk={w.nk}, forward rows ({nbytes / 1e9:.2f} GB)",
+            "value": rows / best, "unit": "operator rows/s", "ms": best * 1e3, "hbm_write_gbs": nbytes / best / 1e9,
+            "kernel": "dense_table_kernel (img2d_plan_dense_table)",
+            "cpu_port": {"value": cpu_nl * w.nf * w.nx / c_s, "unit": "operator rows/s", "cores": 1,
+                         "kind": "port", "sample": f"operators.dense_table (numpy gather), first {cpu_nl} depth steps"},
+            "bitwise_equal_to_host_gather": bool(np.array_equal(head, host))}
+
+
 def workload_config(w, args):
     return {"workload": f"{w.name}: nz={w.nz} nx={w.nx} dx={w.dx} nf={w.nf} taps={w.L} nk={w.nk} ns={w.ns} "
                         f"apertures {int(w.shot_nx.min())}-{int(w.shot_nx.max())} (mean {w.shot_nx.mean():.0f})",
@@ -644,6 +687,10 @@ def main():
             extra["frontend"] = frontend_leg(dev, w)
         except Exception as ex:
             extra["frontend"] = {"error": f"{type(ex).__name__}: {ex}"}
+        try:
+            extra["dense_table"] = dense_table_leg(dev)
+        except Exception as ex:
+            extra["dense_table"] = {"error": f"{type(ex).__name__}: {ex}"}
 
     if rank == 0 and world == 1 and not args.no_lsm:
         try:
