@@ -8,12 +8,13 @@ workload with inputs resident in HBM.  The default workload is `batched_uneven`:
 nx=2048, nf=512 (2-50 Hz), 2M+1=35 taps, nk=4000, 256 shots with apertures U[256, 2048] (seeded
 synthetic data).  Metric: extrapolated points (shot, w, z, x) per second, whole job.
 
-Multi-GPU (torchrun, one rank per GPU): weak scaling; every rank migrates its own shot set of the
-same size and the stacked images are summed with one all-reduce per step.
+Multi-GPU (torchrun, one rank per GPU): weak scaling; every rank migrates the single-GPU survey
+(the same seeded shot set) and the stacked images are summed with one all-reduce per step.
 
 Prints one JSON line (rank 0).  Other modes:
   --impl reference   the reference's own CPU library (oracle/_ref/extrapolation_cpu.so, all host
-                     threads) on a bounded sample of the same workload, same metric.
+                     threads) on a fixed bounded sample of the same workload (ReferenceSample, the
+                     sample of the GPU arm's cpu_baseline leg), same metric and config.
 """
 import argparse
 import json
@@ -55,7 +56,10 @@ def parse_args():
     p.add_argument("--nf", type=int, default=None, help="override frequency count (profiling a reduced case)")
     p.add_argument("--taps", type=int, default=None,
                    help="override the operator length 2M+1 (odd; timing the per-step overhead)")
-    p.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU-baseline sample time")
+    p.add_argument("--cpu-seconds", type=float, default=8.0,
+                   help="reference-library time of the GPU arm's CPU-baseline leg (passes over the fixed sample)")
+    p.add_argument("--ref-step-seconds", type=float, default=2.0,
+                   help="reference-library time per step of --impl reference (passes over the fixed sample)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-naive", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
@@ -154,76 +158,97 @@ class quiet_stdout:
         os.close(self.saved)
 
 
-def reference_sample(w, target_s, max_table_bytes=1 << 30):
-    """Time the reference CPU library on a bounded sample of workload w: the first shots, all
-    frequencies, a leading depth slab; dense tables gathered from the compact table beforehand
-    (not timed, as the reference's EXTRAPOLATION/IMAGING timers exclude table building).
-    Returns (points, seconds, description)."""
-    from oracle import oracle
-    if not oracle.have_ref():
-        raise RuntimeError("oracle/_ref/extrapolation_cpu.so missing")
-    L = w.L
+class ReferenceSample:
+    """A fixed, bounded sample of workload w for the reference's own CPU library
+    (oracle/_ref/extrapolation_cpu.so): `shots` shots at evenly spaced ranks of the aperture widths
+    (narrowest to widest), `freqs` of the frequencies (evenly spaced over the band), the first
+    `depth` depth steps, each shot one call of the reference's `extrapolate` on its own aperture
+    (ns = 1, nx = the aperture width, as the reference handles one geometry per call).  The dense
+    tables are gathered once here and are not timed, as the reference's EXTRAPOLATION and IMAGING
+    timers exclude table building.  The same sample serves the reference arm and the CPU leg of
+    the GPU arm, so the two rates measure the same thing."""
 
-    def run(s, depth):
-        x0, n = int(w.shot_x0[s]), int(w.shot_nx[s])
-        tf = oracle.gather_dense_slab(0, depth, w.nx, x0, n, w.nf, w.M, w.nk, w.dk, w.omega, w.velocity, w.table)
-        tb = oracle.gather_dense_slab(0, depth, w.nx, x0, n, w.nf, w.M, w.nk, w.dk, w.omega, w.velocity, w.table,
-                                      conj_rows=True)
-        wave = np.ascontiguousarray(w.block(w.wave, s)[None])
-        shot = np.ascontiguousarray(w.block(w.shot, s)[None])
-        img = np.zeros((1, depth, n), dtype=np.float32)
+    def __init__(self, w, shots=8, freqs=64, depth=8):
+        from oracle import oracle
+        if not oracle.have_ref():
+            raise RuntimeError("oracle/_ref/extrapolation_cpu.so missing")
+        self.oracle = oracle
+        order = np.argsort(w.shot_nx, kind="stable")
+        pick = order[np.unique(np.linspace(0, len(order) - 1, min(shots, w.ns)).round().astype(int))]
+        jsel = np.unique(np.linspace(0, w.nf - 1, min(freqs, w.nf)).round().astype(int))
+        self.depth = depth = int(min(depth, w.nextrap))
+        self.nf = nf = len(jsel)
+        self.M = w.M
+        self.calls = []
+        for s in pick:
+            x0, n = int(w.shot_x0[s]), int(w.shot_nx[s])
+            om = np.ascontiguousarray(w.omega[jsel])
+            tf = oracle.gather_dense_slab(0, depth, w.nx, x0, n, nf, w.M, w.nk, w.dk, om, w.velocity, w.table)
+            tb = oracle.gather_dense_slab(0, depth, w.nx, x0, n, nf, w.M, w.nk, w.dk, om, w.velocity, w.table,
+                                          conj_rows=True)
+            wave = np.ascontiguousarray(w.block(w.wave, s)[jsel][None])
+            shot = np.ascontiguousarray(w.block(w.shot, s)[jsel][None])
+            self.calls.append((n, tf, tb, wave, shot))
+        self.points = sum(n * nf * depth for n, *_ in self.calls)
+        self.desc = (f"reference extrapolation_cpu.so, {len(self.calls)} shots at evenly spaced ranks of the "
+                     f"aperture widths ({', '.join(str(c[0]) for c in self.calls)} traces), {nf} of {w.nf} "
+                     f"frequencies, first {depth} depth steps, one call per shot; {self.points:.3g} points per "
+                     "pass; dense tables gathered beforehand and not timed")
+
+    def run_pass(self):
+        """One pass over the sample; returns the seconds spent inside the reference's calls."""
+        secs = 0.0
         with quiet_stdout():  # the reference library prints its phase timers on stdout
-            t0 = time.perf_counter()
-            oracle.ref_extrapolate(1, depth, depth, n, w.nf, w.nf, w.M, tf, tb, wave, shot, img)
-            t1 = time.perf_counter()
-        return n * w.nf * depth, t1 - t0
+            for n, tf, tb, wave0, shot0 in self.calls:
+                wave, shot = wave0.copy(), shot0.copy()
+                img = np.zeros((1, self.depth, n), dtype=np.float32)
+                t0 = time.perf_counter()
+                self.oracle.ref_extrapolate(1, self.depth, self.depth, n, self.nf, self.nf, self.M, tf, tb, wave,
+                                            shot, img)
+                secs += time.perf_counter() - t0
+        return secs
 
-    # calibrate on a 2-step slab of shot 0
-    p0, t0 = run(0, 2)
-    rate = p0 / max(t0, 1e-6)
-    order = np.argsort(-w.shot_nx)  # widest first: representative, not cheapest
-    want = rate * target_s
-    pts = 0
-    secs = 0.0
-    used = []
-    for s in order:
-        n = int(w.shot_nx[s])
-        depth = int(min(w.nextrap, max(1, (want - pts) // (n * w.nf)),
-                        max(1, max_table_bytes // (w.nf * n * L * 8))))
-        p, t = run(int(s), depth)
-        pts += p
-        secs += t
-        used.append((int(s), depth))
-        if pts >= want:
-            break
-    desc = (f"reference extrapolation_cpu.so, {len(used)} shot(s) of the workload (widest first), all {w.nf} "
-            f"frequencies, leading depth slabs {[d for _, d in used]}, {pts:.3g} points; dense tables gathered "
-            "beforehand and not timed")
-    return pts, secs, desc
+    def timed(self, seconds):
+        """Passes until `seconds` of reference time have accumulated (at least one); returns
+        (points, seconds)."""
+        pts, secs = 0, 0.0
+        while secs < seconds or pts == 0:
+            secs += self.run_pass()
+            pts += self.points
+        return pts, secs
+
+
+def cpu_threads():
+    return int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
 
 
 def run_reference_impl(args):
+    """The reference arm: the reference's own CPU library on this host's cores, on the fixed sample
+    of the GPU arm's workload (ReferenceSample); one step = passes over the sample for about
+    `--ref-step-seconds` of reference time."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
     from imaging2d_wlsq_b200 import synthetic
-    w = synthetic.WORKLOADS[args.workload](scale=args.scale)
-    rates = []
-    desc = ""
-    t_all = 0.0
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    maker = synthetic.WORKLOADS[args.workload]
+    over = {k: v for k, v in (("nz", args.nz), ("nf", args.nf)) if v}
+    w = maker(scale=args.scale, **over)
+    sample = ReferenceSample(w)
+    pts_all, t_all = 0, 0.0
     for i in range(args.warmup + args.steps):
-        pts, secs, desc = reference_sample(w, max(2.0, args.cpu_seconds / 2))
+        pts, secs = sample.timed(args.ref_step_seconds)
         if i >= args.warmup:
-            rates.append(pts / secs)
+            pts_all += pts
             t_all += secs
-    value = float(np.median(rates))
-    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    value = pts_all / t_all
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t_all / max(1, args.steps),
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c64 (fp32)",
-        "data": "synthetic (seeded)", "config": workload_config(w, args),
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference", "sample": desc},
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c64 (fp32 complex)",
+        "data": "synthetic (seeded)", "config": run_config(w, args, world),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cpu_threads(), "kind": "reference",
+                         "sample": sample.desc},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -448,6 +473,11 @@ def workload_config(w, args):
             "l2": "inputs (wavefields %.2f GB) larger than L2 (126 MB); no flush" % (2 * w.wave.nbytes / 1e9)}
 
 
+def run_config(w, args, world):
+    """The `config` object of both arms' JSON lines (identical for the same workload and N)."""
+    return dict(workload_config(w, args), parallelism=f"shots x{world} (weak)")
+
+
 def main():
     args = parse_args()
     if args.impl == "reference":
@@ -466,10 +496,10 @@ def main():
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
 
-    # weak scaling: each rank its own seeded shot set of the full per-GPU size
+    # weak scaling: every rank migrates the full single-GPU survey (the same seeded shot set as N=1)
     maker = synthetic.WORKLOADS[args.workload]
     over = {k: v for k, v in (("nz", args.nz), ("nf", args.nf)) if v}
-    w = maker(seed=100 + rank, scale=args.scale, **over) if world > 1 else maker(scale=args.scale, **over)
+    w = maker(scale=args.scale, **over)
     if args.taps:
         from imaging2d_wlsq_b200 import operators
         w.M = (args.taps - 1) // 2
@@ -651,10 +681,12 @@ def main():
         # CPU leg: the reference's own library timed on a bounded sample, and the FP64 checker's image
         # of a sub-volume (first 40 depth steps, all shots and frequencies) against this run's kernel
         try:
-            pts, secs, desc = reference_sample(w, args.cpu_seconds)
-            extra["cpu_baseline"] = {"value": pts / secs, "unit": UNIT,
-                                     "cores": int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1)),
-                                     "kind": "reference", "sample": desc}
+            sample = ReferenceSample(w)
+            sample.run_pass()  # warm-up pass (first touch of the library's buffers)
+            pts, secs = sample.timed(args.cpu_seconds)
+            extra["cpu_baseline"] = {"value": pts / secs, "unit": UNIT, "cores": cpu_threads(),
+                                     "kind": "reference", "sample": sample.desc, "seconds": secs}
+            del sample
         except Exception as ex:  # reference library not shipped with this tree
             extra["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
                                      "sample": f"unavailable: {ex}"}
@@ -703,7 +735,7 @@ def main():
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * elapsed / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "c64 (fp32 complex)", "data": "synthetic (seeded)",
-            "config": dict(workload_config(w, args), parallelism=f"shots x{world} (weak)"),
+            "config": run_config(w, args, world),
             "clocks": clk, "gpu_launches": 2 * args.steps,
         }
         line.update(extra)

@@ -108,6 +108,10 @@ def load():
     lib.img2d_plan_describe_demigration.argtypes = [c_void_p, c_char_p, c_int]
     lib.img2d_release_host_cache.restype = None
     lib.img2d_release_host_cache.argtypes = []
+    lib.img2d_host_cache_device_count.restype = c_int
+    lib.img2d_host_cache_device_count.argtypes = []
+    lib.img2d_set_alloc_limit.restype = None
+    lib.img2d_set_alloc_limit.argtypes = [c_size_t]
     lib.img2d_plan_destroy.restype = None
     lib.img2d_plan_destroy.argtypes = [c_void_p]
     return lib

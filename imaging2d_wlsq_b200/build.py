@@ -14,6 +14,8 @@ import sys
 PKG = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(PKG)
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+# read-only mount of the reference sources on the build machine (oracle/_ref recipe input)
+REFERENCE_TREE = "/root/reference"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 LIB = os.path.join(PKG, "libimaging2d_wlsq_b200.so")
 SOURCES = [os.path.join(PKG, "csrc", "wlsq_capi.cu")]
@@ -62,7 +64,12 @@ def build_oracle(force=False):
     ref = os.path.join(ROOT, "oracle", "build_ref.sh")
     ref_out = os.path.join(ROOT, "oracle", "_ref", "extrapolation_cpu.so")
     if force or not os.path.exists(ref_out):
-        _run(["bash", ref])
+        # the reference sources, where the build machine mounts them (absent on machines that
+        # only run the prebuilt files; the recipe then skips)
+        env = dict(os.environ)
+        env.setdefault("IMG2D_REFERENCE", REFERENCE_TREE)
+        print("+ bash", ref, flush=True)
+        subprocess.run(["bash", ref], check=True, env=env)
 
 
 def build_all(force=False):

@@ -3,6 +3,7 @@
 #include <algorithm>
 #include <map>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <numeric>
@@ -309,6 +310,44 @@ __global__ void fma_probe_kernel(float *out, int iters)
 }
 
 // ---------------------------------------------------------------------------------------
+// Device allocation.  Every device buffer the library allocates goes through device_alloc, which
+// refuses (IMG2D_ENOMEM, before calling cudaMalloc) any single allocation larger than the limit set
+// by img2d_set_alloc_limit or, until that is called, by the environment variable
+// IMG2D_ALLOC_LIMIT_BYTES (unset or 0: no limit).  The limit injects allocation failures on the
+// host for tests of the error path, including through the void drop-in shims.
+// ---------------------------------------------------------------------------------------
+static std::mutex g_alloc_mu;
+static bool g_alloc_limit_set = false;
+static size_t g_alloc_limit = 0;
+
+static size_t alloc_limit()
+{
+    std::lock_guard<std::mutex> lock(g_alloc_mu);
+    if (!g_alloc_limit_set) {
+        const char *e = getenv("IMG2D_ALLOC_LIMIT_BYTES");
+        g_alloc_limit = e ? (size_t)strtoull(e, nullptr, 10) : 0;
+        g_alloc_limit_set = true;
+    }
+    return g_alloc_limit;
+}
+
+static int device_alloc(void **p, size_t n)
+{
+    *p = nullptr;
+    const size_t lim = alloc_limit();
+    if (lim && n > lim)
+        return fail(IMG2D_ENOMEM, "device allocation of " + std::to_string(n) + " bytes refused: above the " +
+                                      std::to_string(lim) + "-byte allocation limit (IMG2D_ALLOC_LIMIT_BYTES)");
+    cudaError_t e = cudaMalloc(p, n);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        *p = nullptr;
+        return fail(IMG2D_ENOMEM, "cudaMalloc(" + std::to_string(n) + " bytes): " + cudaGetErrorString(e));
+    }
+    return IMG2D_OK;
+}
+
+// ---------------------------------------------------------------------------------------
 // Plan
 // ---------------------------------------------------------------------------------------
 // Bump allocator over a fixed device region (the no-allocation entry point's static scratch).
@@ -344,14 +383,10 @@ struct DevBuf {
             carver->used = off + n;
             return IMG2D_OK;
         }
-        owned = true;
         if (n == 0) n = 16;
-        cudaError_t e = cudaMalloc(&p, n);
-        if (e != cudaSuccess) {
-            cudaGetLastError();
-            p = nullptr;
-            return fail(IMG2D_ENOMEM, "cudaMalloc(" + std::to_string(n) + " bytes): " + cudaGetErrorString(e));
-        }
+        const int rc = device_alloc(&p, n);
+        if (rc) return rc;
+        owned = true;
         bytes = n;
         return IMG2D_OK;
     }
@@ -975,11 +1010,8 @@ struct Scratch {
     template <class T> int alloc(T **out, size_t n)
     {
         void *q = nullptr;
-        cudaError_t e = cudaMalloc(&q, n ? n : 16);
-        if (e != cudaSuccess) {
-            cudaGetLastError();
-            return fail(IMG2D_ENOMEM, "cudaMalloc(" + std::to_string(n) + " bytes): " + cudaGetErrorString(e));
-        }
+        const int rc = device_alloc(&q, n ? n : 16);
+        if (rc) return rc;
         ptrs.push_back(q);
         *out = static_cast<T *>(q);
         return IMG2D_OK;
@@ -1056,16 +1088,20 @@ static int run_dense(int ns, int nextrap, int nz, int nx, int nf, int nt, int M,
     return IMG2D_OK;
 }
 
-// One cached plan for the host compact entry point, reused while the geometry is unchanged, and
-// its device buffers, kept between calls (grown on demand) so a call allocates nothing when the
-// sizes repeat.
-static std::mutex g_cache_mu;
-static img2d_plan *g_cached = nullptr;
-static std::vector<int> g_cached_key;
+// Per device: one cached plan for the host compact entry point, reused while the geometry is
+// unchanged, and its device buffers, kept between calls (grown on demand) so a call allocates
+// nothing when the sizes repeat.  Everything in an entry belongs to that device and is only used
+// (and freed) while it is the current device.
 struct HostEntryBuffers {
     DevBuf omega, vel, tabF, tabB, wave, shot, image, image_shots;
 };
-static HostEntryBuffers *g_host_bufs = nullptr;
+struct HostCache {
+    img2d_plan *plan = nullptr;
+    std::vector<int> key;
+    HostEntryBuffers *bufs = nullptr;
+};
+static std::mutex g_cache_mu;
+static std::map<int, HostCache> g_host_cache;
 
 }  // namespace img2d
 
@@ -1104,6 +1140,13 @@ using namespace img2d;
 extern "C" {
 
 const char *img2d_last_error(void) { return g_err.c_str(); }
+
+void img2d_set_alloc_limit(size_t max_bytes)
+{
+    std::lock_guard<std::mutex> lock(g_alloc_mu);
+    g_alloc_limit = max_bytes;
+    g_alloc_limit_set = true;
+}
 
 int img2d_version(void) { return 10000; }
 
@@ -1557,11 +1600,25 @@ int img2d_migrate_compact_noalloc(int ns, int nextrap, int nz, int nx, int nf, i
 void img2d_release_host_cache(void)
 {
     std::lock_guard<std::mutex> lock(g_cache_mu);
-    delete g_cached;
-    g_cached = nullptr;
-    g_cached_key.clear();
-    delete g_host_bufs;
-    g_host_bufs = nullptr;
+    int cur = -1;
+    if (cudaGetDevice(&cur) != cudaSuccess) {
+        cudaGetLastError();
+        cur = -1;
+    }
+    for (auto &kv : g_host_cache) {
+        // free each device's plan and buffers with that device current
+        if (cudaSetDevice(kv.first) != cudaSuccess) cudaGetLastError();
+        delete kv.second.plan;
+        delete kv.second.bufs;
+    }
+    g_host_cache.clear();
+    if (cur >= 0 && cudaSetDevice(cur) != cudaSuccess) cudaGetLastError();
+}
+
+int img2d_host_cache_device_count(void)
+{
+    std::lock_guard<std::mutex> lock(g_cache_mu);
+    return (int)g_host_cache.size();
 }
 
 int img2d_migrate_compact(int ns, int nextrap, int nz, int nx, int nf, int nt, int M, int nk, double dk,
@@ -1575,23 +1632,26 @@ int img2d_migrate_compact(int ns, int nextrap, int nz, int nx, int nf, int nt, i
         return fail(IMG2D_EINVAL, "null pointer argument");
     if ((flags & IMG2D_FLAG_TWO_TABLES) && !tab_back) return fail(IMG2D_EINVAL, "two-table mode needs tab_back");
     std::lock_guard<std::mutex> lock(g_cache_mu);
+    int dev = 0;
+    IMG2D_CUDA(cudaGetDevice(&dev));
+    HostCache &hc = g_host_cache[dev];
     std::vector<int> key = {ns, nextrap, nz, nx, nf, nt, M, nk, flags};
     for (int s = 0; s < ns; ++s) {
         key.push_back(shot_x0 ? shot_x0[s] : 0);
         key.push_back(shot_nx ? shot_nx[s] : nx);
     }
-    if (!g_cached || key != g_cached_key) {
-        delete g_cached;
-        g_cached = nullptr;
-        g_cached_key.clear();
+    if (!hc.plan || key != hc.key) {
+        delete hc.plan;
+        hc.plan = nullptr;
+        hc.key.clear();
         img2d_plan *p = nullptr;
         if ((rc = img2d_plan_create(&p, ns, nextrap, nz, nx, nf, nt, M, nk, shot_x0, shot_nx, flags))) return rc;
-        g_cached = p;
-        g_cached_key = key;
+        hc.plan = p;
+        hc.key = key;
     }
-    img2d_plan *p = g_cached;
-    if (!g_host_bufs) g_host_bufs = new HostEntryBuffers();
-    HostEntryBuffers &hb = *g_host_bufs;
+    img2d_plan *p = hc.plan;
+    if (!hc.bufs) hc.bufs = new HostEntryBuffers();
+    HostEntryBuffers &hb = *hc.bufs;
     const size_t L = 2 * (size_t)M + 1;
     const size_t plane = (size_t)nz * nx;
     if ((rc = hb.omega.ensure(nf * sizeof(double)))) return rc;

@@ -3,7 +3,7 @@
  *
  * Library: imaging2d_wlsq_b200/libimaging2d_wlsq_b200.so (CUDA, sm_100a).
  * Drop-in shims with the reference's library names and its void `extrapolate` symbols are
- * built into imaging2d_wlsq_b200/dropin/ (see INTEGRATION.md).
+ * built into imaging2d_wlsq_b200/dropin/ (csrc/dropin.c).
  *
  * Data conventions shared by every entry point:
  *   img2d_c64   interleaved (re, im) float32 pair, the layout of numpy.complex64 and of the
@@ -47,6 +47,13 @@ typedef struct {
 
 const char *img2d_last_error(void);
 int img2d_version(void);
+
+/* Failure injection for tests of the error path (no counterpart in the reference, which checks no
+ * allocation).  Every device allocation of the library larger than max_bytes then fails with
+ * IMG2D_ENOMEM on the host, before cudaMalloc is called; 0 removes the limit.  Until this is
+ * called the limit comes from the environment variable IMG2D_ALLOC_LIMIT_BYTES (unset: none), so
+ * it also reaches callers of the void drop-in shims, which then print the error and abort. */
+void img2d_set_alloc_limit(size_t max_bytes);
 
 /* ------------------------------------------------------------------------------------------
  * Drop-in entry points: the reference's dense-table ABI.
@@ -92,9 +99,12 @@ int img2d_migrate_compact(int ns, int nextrap, int nz, int nx, int nf, int nt, i
                           const img2d_c64 *tab_forw, const img2d_c64 *tab_back,
                           const int *shot_x0, const int *shot_nx, img2d_c64 *wave_fs,
                           img2d_c64 *shot_fs, float *image, float *image_shots, int flags);
-/* img2d_migrate_compact keeps its plan (for the last geometry) and its device buffers (grown to the
- * largest sizes seen) between calls, so repeated calls allocate nothing.  This frees them. */
+/* img2d_migrate_compact keeps, per device, its plan (for the last geometry on that device) and its
+ * device buffers (grown to the largest sizes seen) between calls, so repeated calls allocate
+ * nothing.  img2d_release_host_cache frees them on every device; img2d_host_cache_device_count
+ * is the number of devices that hold such a cache. */
 void img2d_release_host_cache(void);
+int img2d_host_cache_device_count(void);
 
 /* ------------------------------------------------------------------------------------------
  * Plan interface for device-resident data (the building block under the host entry points).
@@ -183,8 +193,10 @@ int img2d_records_to_spectra(int ns, int nt, int nx, int nf, int nt_rows, const 
  *  - All calls share the one array and it keeps the last call's contents (the entry point
  *    clears what must start at zero).  Calls that overlap on the GPU race: issue them on one
  *    stream, or wait for the previous call before the next.
- *  - Asynchronous on `stream` except for a short upload of the work descriptors, after which the
- *    call waits for that stream.
+ *  - Every call copies its work descriptors from pageable host memory to the array with
+ *    cudaMemcpyAsync on `stream` and then calls cudaStreamSynchronize(stream), so it returns only
+ *    after the work queued on `stream` before it has finished; the index-table build, the
+ *    migration and the image reduction that follow are queued on `stream` without waiting.
  * ---------------------------------------------------------------------------------------- */
 #define IMG2D_NOALLOC_SCRATCH_BYTES (64ull << 20)
 int img2d_migrate_compact_noalloc(int ns, int nextrap, int nz, int nx, int nf, int nt, int M, int nk,

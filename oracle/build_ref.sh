@@ -6,7 +6,11 @@
 # ref_shim/ supplies the two MKL CBLAS calls and zeroed operator new[] (see ref_shim.cpp).
 set -euo pipefail
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
-REF="${IMG2D_REFERENCE:-/root/reference}"
+REF="${IMG2D_REFERENCE:-}"
+if [ -z "$REF" ]; then
+  echo "IMG2D_REFERENCE (the reference source tree) is not set; skipping oracle/_ref build" >&2
+  exit 0
+fi
 OUT="$HERE/_ref"
 if [ ! -f "$REF/cpp_src/extrapolation_cpu.cpp" ]; then
   echo "reference sources not found at $REF; skipping oracle/_ref build" >&2

@@ -1,9 +1,9 @@
 """Generate the golden fixtures in tests/golden/ from the reference implementation.
 
-Run on a machine that has the reference sources (default /root/reference, override with
-IMG2D_REFERENCE) and the reference CPU library built by oracle/build_ref.sh:
+Run on a machine that has the reference sources (their root in IMG2D_REFERENCE) and the reference
+CPU library built by oracle/build_ref.sh:
 
-    python tests/golden/make_golden.py
+    IMG2D_REFERENCE=<reference source tree> python tests/golden/make_golden.py
 
 Writes
   operators_small.npz  outputs of the reference's own Python operator design
@@ -34,7 +34,9 @@ import sys
 
 import numpy as np
 
-REF = os.environ.get("IMG2D_REFERENCE", "/root/reference")
+REF = os.environ.get("IMG2D_REFERENCE")
+if not REF:
+    sys.exit("set IMG2D_REFERENCE to the reference source tree")
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, os.path.join(REF, "py_src", "operatorsPreparation"))

@@ -7,7 +7,7 @@ import sys
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 CMD = [sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "1", "--warmup", "3",
-       "--scale", "0.05", "--cpu-seconds", "1"]
+       "--scale", "0.05", "--ref-step-seconds", "0.2"]
 
 
 def _run(env_extra=None):
@@ -26,6 +26,9 @@ def test_reference_arm_prints_one_json_line():
     assert d["cpu_baseline"]["kind"] == "reference" and d["cpu_baseline"]["cores"] >= 1
     assert d["e2e"] == {"value": d["value"], "unit": "pts/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
     assert d["config"]["workload"].startswith("batched_uneven")
+    # the same config object as the GPU arm's line (bench.run_config), parallelism included
+    assert d["config"]["parallelism"] == "shots x1 (weak)"
+    assert "shots at evenly spaced ranks" in d["cpu_baseline"]["sample"]
 
 
 def test_reference_arm_other_ranks_do_no_work():

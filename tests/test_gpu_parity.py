@@ -317,3 +317,29 @@ def test_wide_window_non_portable_cluster():
     assert d["kernel"] == "migrate_cluster2" and d["cluster"] == 12, d
     img, _, wave, shot = migration.migrate_workload(w)
     _compact_check(w, img, wave, shot)
+
+
+@pytest.mark.skipif(not oracle.have_ref(), reason="oracle/_ref/extrapolation_cpu.so not built")
+def test_plain_small_in_full_through_dense_dropin_matches_reference_library():
+    """The plain small configuration in full (nz=200, nx=320, nf=64 over 2-30 Hz, 25 taps, 4
+    full-aperture shots; dense tables 200 x 64 x 320 x 25) through the drop-in
+    `extrapolation_cpu.so`, bound as cpp_src/interface.py binds it, against the reference's own
+    extrapolation_cpu.so on the same dense tables and spectra, and against the FP64 oracle."""
+    w = synthetic.plain_small()
+    ns, nl, nz, nx, nf, M = w.ns, w.nextrap, w.nz, w.nx, w.nf, w.M
+    tf = oracle.gather_dense_slab(0, nl, nx, 0, nx, nf, M, w.nk, w.dk, w.omega, w.velocity, w.table)
+    tb = oracle.gather_dense_slab(0, nl, nx, 0, nx, nf, M, w.nk, w.dk, w.omega, w.velocity, w.table,
+                                  conj_rows=True)
+    wave0 = w.wave.reshape(ns, nf, nx)
+    shot0 = w.shot.reshape(ns, nf, nx)
+    img_r = np.zeros((ns, nz, nx), dtype=np.float32)
+    wr, sr = wave0.copy(), shot0.copy()
+    oracle.ref_extrapolate(ns, nl, nz, nx, nf, nf, M, tf, tb, wr, sr, img_r)
+    img_g = np.zeros((ns, nz, nx), dtype=np.float32)
+    wg, sg = wave0.copy(), shot0.copy()
+    _dropin("extrapolation_cpu.so")(ns, nl, nz, nx, nf, nf, M, tf, tb, wg, sg, img_g)
+    assert rel_l2(img_g, img_r) <= 1e-5
+    assert rel_l2(wg, wr) <= 1e-5 and rel_l2(sg, sr) <= 1e-5
+    _, shots64, w64, s64 = oracle.migrate_workload_f64(w)
+    assert rel_l2(img_g, shots64) <= 1e-5
+    assert rel_l2(wg.reshape(-1), w64) <= 1e-5 and rel_l2(sg.reshape(-1), s64) <= 1e-5

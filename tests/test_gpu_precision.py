@@ -41,8 +41,9 @@ def test_precision_modes_small():
 
 def test_precision_study_subvolume():
     """The precision configuration's grid (nx=4096, dx=dz=5 m, 55 taps, nk=8000, thin layers)
-    on a 200-depth-step sub-volume, 16 shots x 16 frequencies spread over 2-60 Hz."""
-    w = synthetic.precision(nextrap=200, nf=16, ns=16)
+    on a 200-depth-step sub-volume with all 64 full-aperture shots and 64 frequencies spread over
+    2-60 Hz (3.4e9 points; the FP64 oracle takes a few minutes of host time)."""
+    w = synthetic.precision(nextrap=200, nf=64, ns=64)
     res = precision.study(w, _fp64)
     _report("subvolume_200", res)
     assert res["fp32"]["accepted"], res

@@ -5,9 +5,10 @@ inside a host application whose own pool owns all device memory, or a processing
 not block on or fail in an allocation mid-run.  Its scratch is one fixed array inside the library.
 
 Checked here through the C ABI: two calls in a row give the same image and wavefields as the
-plan entry point (img2d_plan_execute) within the compact-path tolerance (relative L2 1e-5), the
-second call is not disturbed by what the first left in the shared scratch, and a problem whose
-scratch does not fit is refused with a message naming the limit.  The file is collected last so
+plan entry point (img2d_plan_execute) and as the FP64 CPU oracle, within the compact-path
+tolerance (relative L2 1e-5); the second call is not disturbed by what the first left in the
+shared scratch; and a problem whose scratch does not fit is refused with a message naming the
+limit.  The file is collected last so
 that a failure here does not hide the other tests; it also passes run alone in a fresh process.
 """
 import ctypes
@@ -16,6 +17,7 @@ import numpy as np
 import pytest
 
 from imaging2d_wlsq_b200 import _lib, migration, synthetic
+from oracle import oracle
 from tests.conftest import rel_l2
 
 pytestmark = pytest.mark.gpu
@@ -64,10 +66,15 @@ def test_noalloc_matches_plan_entry_two_calls(maker, kw):
         results.append((img.cpu().numpy(), wave.cpu().numpy(), shot.cpu().numpy()))
 
     ref_img = img_p.cpu().numpy()
+    stack64, _, wave64, shot64 = oracle.migrate_workload_f64(w)
     for img, wave, shot in results:
         assert rel_l2(img[:w.nextrap], ref_img[:w.nextrap]) <= 1e-5
         assert rel_l2(wave, wave_p.cpu().numpy()) <= 1e-5
         assert rel_l2(shot, shot_p.cpu().numpy()) <= 1e-5
+        # and directly against the FP64 oracle
+        assert rel_l2(img[:w.nextrap], stack64[:w.nextrap]) <= 1e-5
+        assert rel_l2(wave, wave64) <= 1e-5
+        assert rel_l2(shot, shot64) <= 1e-5
         assert np.all(img[w.nextrap:] == 7.0)  # rows below nextrap are not touched
     assert rel_l2(results[1][0], results[0][0]) <= 1e-5
 
