@@ -49,7 +49,10 @@ def parse_args():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--workload", default="batched_uneven")
     p.add_argument("--scale", type=float, default=1.0)
-    p.add_argument("--e2e-steps", type=int, default=2)
+    p.add_argument("--e2e-steps", type=int, default=0, help="end-to-end calls timed (0: as many as --steps)")
+    p.add_argument("--strong", action="store_true",
+                   help="strong scaling: the ranks split one survey's shots (sharding.migrate_sharded's "
+                        "decomposition) instead of each migrating the whole survey")
     p.add_argument("--variant", type=int, default=0, help="cluster-kernel variant (1-based; 0 = default)")
     p.add_argument("--no-autotune", action="store_true", help="use the plan's default kernel configuration")
     p.add_argument("--nz", type=int, default=None, help="override depth steps (profiling a reduced case)")
@@ -245,8 +248,8 @@ def run_reference_impl(args):
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t_all / max(1, args.steps),
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c64 (fp32 complex)",
-        "data": "synthetic (seeded)", "config": run_config(w, args, world),
+        "higher_is_better": True, "scaling": scaling(args, world), "vs_baseline": None,
+        "dtype": "c64 (fp32 complex)", "data": "synthetic (seeded)", "config": run_config(w, args, world),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cpu_threads(), "kind": "reference",
                          "sample": sample.desc},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -473,9 +476,13 @@ def workload_config(w, args):
             "l2": "inputs (wavefields %.2f GB) larger than L2 (126 MB); no flush" % (2 * w.wave.nbytes / 1e9)}
 
 
+def scaling(args, world):
+    return "strong" if (args.strong and world > 1) else "weak"
+
+
 def run_config(w, args, world):
     """The `config` object of both arms' JSON lines (identical for the same workload and N)."""
-    return dict(workload_config(w, args), parallelism=f"shots x{world} (weak)")
+    return dict(workload_config(w, args), parallelism=f"shots x{world} ({scaling(args, world)})")
 
 
 def main():
@@ -486,6 +493,7 @@ def main():
     import torch
     import torch.distributed as dist
     from imaging2d_wlsq_b200 import migration, synthetic
+    from imaging2d_wlsq_b200.sharding import sum_images_f64 as sharding_sum
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -504,6 +512,11 @@ def main():
         from imaging2d_wlsq_b200 import operators
         w.M = (args.taps - 1) // 2
         w.table = operators.design_compact_table(w.nx, w.dx, w.dz, w.M, w.nk, w.dk)
+    survey = w
+    if args.strong and world > 1:
+        # strong scaling: this rank's LPT share of the survey's shots
+        from imaging2d_wlsq_b200 import sharding
+        w = sharding.sub_workload(survey, sharding.assign_shots(survey.shot_nx, world)[rank])
     om = torch.from_numpy(w.omega).to(dev)
     vel = torch.from_numpy(np.ascontiguousarray(w.velocity)).to(dev)
     tab = torch.from_numpy(w.table).to(dev)
@@ -531,7 +544,8 @@ def main():
         shot.copy_(shot0)
         plan.execute(wave, shot, image)
         if world > 1:
-            dist.all_reduce(image)
+            # the stacked image over all ranks, reduced in float64 (sharding.sum_images_f64)
+            image.copy_(sharding_sum(image))
 
     for _ in range(args.warmup):
         step()
@@ -558,7 +572,7 @@ def main():
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     elapsed = float(t.item())
-    total_pts = pts_rank * world
+    total_pts = survey.points() if (args.strong and world > 1) else pts_rank * world
     value = total_pts * args.steps / elapsed
     k_s = float(np.mean(kernel_ms)) / 1e3
     describe = plan.describe()
@@ -633,7 +647,7 @@ def main():
             return ta.elapsed_time(tb) / 1e3
 
         e2e_call()
-        secs = [e2e_call() for _ in range(max(1, args.e2e_steps))]
+        secs = [e2e_call() for _ in range(max(1, args.e2e_steps or args.steps))]
         h2d = w.wave.nbytes + w.shot.nbytes + w.omega.nbytes + w.nextrap * w.nx * 8 + w.table.nbytes
         d2h = w.wave.nbytes + w.shot.nbytes + w.nextrap * w.nx * 4
         extra["e2e"] = {"value": pts_rank / float(np.median(secs)), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
@@ -734,8 +748,8 @@ def main():
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * elapsed / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "c64 (fp32 complex)", "data": "synthetic (seeded)",
-            "config": run_config(w, args, world),
+            "scaling": scaling(args, world), "vs_baseline": None, "dtype": "c64 (fp32 complex)",
+            "data": "synthetic (seeded)", "config": run_config(survey, args, world),
             "clocks": clk, "gpu_launches": 2 * args.steps,
         }
         line.update(extra)

@@ -15,8 +15,8 @@ Writes
                        the first nw rows of scipy.fftpack.fft of that record (the receiver spectra the
                        demo feeds to the extrapolation); the source spectra of all shots are in
                        demo_case.npz
-  driver_case.npz      inputs of the reference driver for two demo shots (the raw velocity model, the
-                       two time-domain CSV records and their source indices) and the image that the
+  driver_case.npz      inputs of the reference driver for all nine demo shots (the raw velocity model,
+                       the time-domain CSV records and their source indices) and the image that the
                        reference flow (main.py: its Python operator design and data preparation, then
                        oracle/_ref/extrapolation_cpu.so on the dense tables) produces from them
   demo_case.npz        the reference demo (demo-data/, problemSetup.txt) reduced to the compact form
@@ -167,7 +167,7 @@ def frontend_case():
                         wavelet_t=wavelet, rec_t=rec, rec_f=rec_f.astype(np.complex64))
 
 
-def driver_case(nshots=2):
+def driver_case(nshots=None):
     vel0 = np.genfromtxt(os.path.join(REF, "demo-data", "velmod.csv"), delimiter=",")
     vel = 1.0 / ndimage.gaussian_filter(1.0 / vel0, sigma=2)     # main.py:40-41
     cfg = parse_setup(os.path.join(REF, "demo-data", "problemSetup.txt"))
@@ -190,7 +190,8 @@ def driver_case(nshots=2):
                                    prep.makeForwPSoperators(kappa, kx, dz))       # main.py:82-88
     tb = prep.makeTableOfOperators(nextrap, nx, nw, kappa, kx, w, vel, gidx, op,
                                    prep.makeBackPSoperators(kappa, kx, dz))
-    files = glob.glob(os.path.join(REF, "demo-data", "seismicShots") + "/*.csv")[:nshots]
+    files = sorted(glob.glob(os.path.join(REF, "demo-data", "seismicShots") + "/*.csv"))[:nshots]
+    nshots = len(files)
     isx = [int(re.search(r"seis(.+?)_", os.path.basename(f)).group(1)) for f in files]
     v = vel[0, 0]
     tj = [j * dt for j in range(nt)]
@@ -210,8 +211,8 @@ def driver_case(nshots=2):
 
 
 if __name__ == "__main__":
-    operators_small()
-    frontend_case()
-    driver_case()
-    demo_case()
+    # all fixtures, or only those named on the command line (e.g. `make_golden.py driver_case`)
+    makers = {f.__name__: f for f in (operators_small, frontend_case, driver_case, demo_case)}
+    for name in sys.argv[1:] or list(makers):
+        makers[name]()
     print("wrote", os.listdir(HERE))

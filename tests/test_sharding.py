@@ -70,3 +70,51 @@ def test_two_gloo_ranks_reproduce_single_process_image():
     w = synthetic.batched_uneven(scale=0.05)
     ref, _, _, _ = oracle.migrate_workload_f64(w)
     assert np.linalg.norm(got - ref) / np.linalg.norm(ref) < 1e-12
+
+
+def _oracle_migrate(sub):
+    """A rank's share migrated by the FP64 CPU oracle (stands in for the GPU plan on gloo ranks)."""
+    stack, _, wo, so = oracle.migrate_workload_f64(sub)
+    return (torch.from_numpy(stack.astype(np.float32)), torch.from_numpy(wo.astype(np.complex64)),
+            torch.from_numpy(so.astype(np.complex64)))
+
+
+def _sharded_rank(rank, world, port, q):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    import datetime
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    w = synthetic.batched_uneven(scale=0.05)
+    img, mine, wave, shot = sharding.migrate_sharded(w, migrate_fn=_oracle_migrate)
+    q.put((rank, img.numpy(), mine, wave.numpy(), shot.numpy()))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_migrate_sharded_two_gloo_ranks_strong_scaling():
+    """One survey over two ranks through sharding.migrate_sharded: the shots are partitioned, every
+    rank gets the same stacked image (float64 cross-rank sum), equal to the single-process image,
+    and each rank's final wavefields are those of its own shots."""
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_sharded_rank, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    got = [q.get(timeout=120) for _ in range(2)]
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    got.sort(key=lambda g: g[0])
+    w = synthetic.batched_uneven(scale=0.05)
+    ref, _, wo, so = oracle.migrate_workload_f64(w)
+    np.testing.assert_array_equal(got[0][1], got[1][1])
+    assert np.linalg.norm(got[0][1] - ref) / np.linalg.norm(ref) < 1e-6
+    owned = np.sort(np.concatenate([g[2] for g in got]))
+    np.testing.assert_array_equal(owned, np.arange(w.ns))
+    off = w.offsets()
+    for _, _, mine, wave, shot in got:
+        exp_w = np.concatenate([wo[off[s]:off[s] + w.nf * w.shot_nx[s]] for s in mine])
+        exp_s = np.concatenate([so[off[s]:off[s] + w.nf * w.shot_nx[s]] for s in mine])
+        assert np.abs(wave - exp_w).max() <= 1e-6 * np.abs(exp_w).max()
+        assert np.abs(shot - exp_s).max() <= 1e-6 * np.abs(exp_s).max()
