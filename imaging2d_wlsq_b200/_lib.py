@@ -29,6 +29,8 @@ SOURCE_RECOMPUTE, SOURCE_KEEP, SOURCE_REUSE = 0, 1, 2
 FLAG_TABLE_FP16 = 16
 FLAG_TABLE_BF16 = 32
 FLAG_DEMIG_NO_RING = 64
+FLAG_WIDE = 128
+FLAG_WIDE_SCALAR = 1 << 16
 NOALLOC_SCRATCH_BYTES = 64 << 20
 
 ERROR_NAMES = {1: "EINVAL", 2: "ENOMEM", 3: "ECUDA", 4: "ENODEV"}

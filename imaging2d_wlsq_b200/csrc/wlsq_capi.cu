@@ -15,6 +15,7 @@
 #include "wlsq_kernels.cuh"
 #include "wlsq_cluster.cuh"
 #include "wlsq_cluster2.cuh"
+#include "wlsq_wide.cuh"
 #include "wlsq_adjoint.cuh"
 #include "wlsq_adjoint_cluster.cuh"
 #include "wlsq_frontend.cuh"
@@ -652,11 +653,32 @@ static int build_plan(img2d_plan *p, int ns, int nextrap, int nz, int nx, int nf
         p->kname = "migrate_cluster2";
         return true;
     };
-    if (cluster_ok && !(flags & IMG2D_FLAG_CLUSTER_V1) && p->L >= 7) {
+    if (cluster_ok && !(flags & (IMG2D_FLAG_CLUSTER_V1 | IMG2D_FLAG_WIDE)) && p->L >= 7) {
         // the default ring variant needs 33 KB more shared memory than the staged one: long
         // operators or very wide windows fall back to the staged variant
         if (!try_cluster2(cv, vsel) && !explicit_variant && !tab16 && vsel != kCluster2Staged)
             try_cluster2(kCluster2[kCluster2Staged], kCluster2Staged);
+    }
+    // Wide cluster kernel (8 slots x 1024 positions per CTA, clusters of half the size): on request
+    if (!p->cluster && !tab16 && mode == OP_CONJ && (flags & IMG2D_FLAG_WIDE) &&
+        !(flags & (IMG2D_FLAG_GENERIC | IMG2D_FLAG_NO_CLUSTER)) && p->L >= 7) {
+        const KernelFn wf = (flags & IMG2D_FLAG_WIDE_SCALAR) ? migrate_wide_kernel<0> : migrate_wide_kernel<1>;
+        const size_t smemw = wide_smem_bytes(M);
+        if (smemw + static_reserve <= (size_t)smem_optin) {
+            const int widest = make_groups(WideShape::G);
+            const int K = (widest + WideShape::PC - 1) / WideShape::PC;
+            if (K <= 8 || (K <= kMaxCluster && clusters_that_fit((const void *)wf, K, WideShape::NW * 32, smemw) > 0)) {
+                p->cluster = K;
+                p->G = WideShape::G;
+                p->fixed = true;
+                p->fn = wf;
+                p->smem = smemw;
+                p->max_w = widest;
+                p->block = WideShape::NW * 32;
+                p->variant = (flags & IMG2D_FLAG_WIDE_SCALAR) ? 0 : 1;
+                p->kname = "migrate_wide";
+            }
+        }
     }
     if (tab16 && !p->cluster)
         return fail(IMG2D_EINVAL, "16-bit operator tables need the cluster kernel (>= 12 lane slots, 2M+1 >= 7, "

@@ -41,6 +41,8 @@ typedef struct {
 #define IMG2D_FLAG_TABLE_FP16 16  /* operator table stored as FP16 (re, im) pairs, arithmetic FP32 */
 #define IMG2D_FLAG_TABLE_BF16 32  /* operator table stored as BF16 (re, im) pairs, arithmetic FP32 */
 #define IMG2D_FLAG_DEMIG_NO_RING 64 /* demigration: forward steps read operator pairs through L1, not the ring */
+#define IMG2D_FLAG_WIDE 128        /* wide cluster kernel: 8 slots x 1024 positions per CTA (packed FMAs) */
+#define IMG2D_FLAG_WIDE_SCALAR (1 << 16) /* with IMG2D_FLAG_WIDE: scalar instead of packed FMAs */
 /* select variant v (1-based; 0 = default) of the second-generation cluster kernel: bits 8-15 */
 #define IMG2D_FLAG_VARIANT_SHIFT 8
 #define IMG2D_FLAG_VARIANT(v) ((v) << IMG2D_FLAG_VARIANT_SHIFT)

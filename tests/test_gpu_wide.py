@@ -1,0 +1,89 @@
+"""The wide cluster kernel (8 lane slots x 1024 positions per CTA, clusters of half the size of the
+cluster2 kernel's) against the FP64 oracle (relative L2 1e-5, the compact-path bar), in both its
+packed (FFMA2) and scalar FMA forms, and bit for bit against the cluster2 kernel's final wavefields
+(the same FMA sequence per element)."""
+import numpy as np
+import pytest
+
+from imaging2d_wlsq_b200 import migration, operators, synthetic
+from oracle import oracle
+from tests.conftest import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+ARITH = [dict(wide=True), dict(wide_scalar=True)]
+
+
+def _with_M(w, M):
+    w.M = M
+    w.table = operators.design_compact_table(w.nx, w.dx, w.dz, M, w.nk, w.dk)
+    return w
+
+
+CASES = {
+    "uneven_L35": lambda: synthetic.batched_uneven(scale=0.12),
+    "medium_L31": lambda: synthetic.plain_medium(scale=0.125),
+    "precision_L55": lambda: synthetic.precision(scale=0.05),
+    "small_L25": lambda: synthetic.plain_small(scale=0.5),
+    "uneven_L7": lambda: _with_M(synthetic.batched_uneven(nx=700, nz=10, nf=3, ns=40), 3),
+    "uneven_L81": lambda: _with_M(synthetic.batched_uneven(nx=700, nz=10, nf=3, ns=40), 40),
+    # windows wider than one cluster of 2: K = 3 (2600 positions) and K = 5 (4500 positions)
+    "wide_K3": lambda: synthetic.batched_uneven(nx=2600, nz=6, nf=2, ns=24),
+    "wide_K5": lambda: synthetic.plain_medium(nx=4500, nz=5, nf=2, ns=6),
+}
+
+
+@pytest.mark.parametrize("case", list(CASES))
+@pytest.mark.parametrize("arith", ARITH, ids=["ffma2", "ffma"])
+def test_wide_matches_fp64_oracle(case, arith):
+    w = CASES[case]()
+    d = migration.Plan.for_workload(w, **arith).describe()
+    assert d["kernel"] == "migrate_wide" and d["G"] == 8, d
+    img, _, wave, shot = migration.migrate_workload(w, **arith)
+    stack, _, wo, so = oracle.migrate_workload_f64(w)
+    assert rel_l2(img, stack) <= 1e-5
+    assert rel_l2(wave, wo) <= 1e-5 and rel_l2(shot, so) <= 1e-5
+    assert np.all(img[w.nextrap:] == 0)
+
+
+@pytest.mark.parametrize("arith", ARITH, ids=["ffma2", "ffma"])
+def test_wide_wavefields_bitwise_equal_cluster2(arith):
+    w = synthetic.batched_uneven(scale=0.1)
+    assert migration.Plan.for_workload(w).describe()["kernel"] == "migrate_cluster2"
+    _, _, wave_c, shot_c = migration.migrate_workload(w)
+    _, _, wave_w, shot_w = migration.migrate_workload(w, **arith)
+    np.testing.assert_array_equal(wave_w, wave_c)
+    np.testing.assert_array_equal(shot_w, shot_c)
+
+
+def test_wide_per_shot_images():
+    w = synthetic.batched_uneven(scale=0.08)
+    img, imgs, wave, shot = migration.migrate_workload(w, image_shots=True, wide=True)
+    _, shots_o, _, _ = oracle.migrate_workload_f64(w)
+    assert rel_l2(imgs, shots_o) <= 1e-5
+    for s in range(w.ns):
+        x0, n = int(w.shot_x0[s]), int(w.shot_nx[s])
+        assert np.all(imgs[s, :, :x0] == 0) and np.all(imgs[s, :, x0 + n:] == 0)
+    assert rel_l2(imgs.sum(axis=0), img) <= 1e-6
+
+
+def test_wide_device_plan_repeat_and_rows_beyond_nextrap():
+    import torch
+    w = synthetic.batched_uneven(scale=0.08)
+    w.nextrap = w.nz - 3
+    dev = torch.device("cuda")
+    plan = migration.Plan.for_workload(w, wide=True)
+    plan.set_model(torch.from_numpy(w.omega).to(dev), torch.from_numpy(np.ascontiguousarray(w.velocity)).to(dev),
+                   w.dk, torch.from_numpy(w.table).to(dev))
+    stack, _, wo, _ = oracle.migrate_workload_f64(w)
+    for _ in range(2):
+        wave = torch.from_numpy(w.wave.copy()).to(dev)
+        shot = torch.from_numpy(w.shot.copy()).to(dev)
+        img = torch.full((w.nz, w.nx), 5.0, dtype=torch.float32, device=dev)
+        plan.execute(wave, shot, img)
+        torch.cuda.synchronize()
+        got = img.cpu().numpy()
+        assert rel_l2(got[:w.nextrap], stack[:w.nextrap]) <= 1e-5
+        assert np.all(got[w.nextrap:] == 5.0)
+        assert rel_l2(wave.cpu().numpy(), wo) <= 1e-5
+    plan.close()
