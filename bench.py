@@ -72,8 +72,8 @@ def parse_args():
     p.add_argument("--no-frontend", action="store_true", help="skip the front-end (wavelet, record spectra) leg")
     p.add_argument("--no-accuracy", action="store_true",
                    help="skip the rel-L2 check of the image against the FP64 checker on a sub-volume")
-    p.add_argument("--kernel", default="auto", choices=["auto", "cluster1", "single"],
-                   help="kernel family (comparison runs); auto = the plan's choice")
+    p.add_argument("--kernel", default="auto", choices=["auto", "cluster2", "wide", "wide-scalar", "cluster1", "single"],
+                   help="kernel family (comparison runs and profiling); auto = the autotuner's choice")
     return p.parse_args()
 
 
@@ -293,7 +293,8 @@ def lsm_leg(dev, iters, scale=1.0):
     e1.synchronize()
     t_mig = e0.elapsed_time(e1) / 1e3
     pts = w.points()
-    dots = [lsm.dot_product_test(op, seed=sd) for sd in range(3)]
+    dots = [lsm.dot_product_test(op, seed=sd) for sd in range(5)]
+    dots_sep = [lsm.dot_product_test(op, seed=sd, separation=3.0) for sd in range(5)]
     rng = np.random.default_rng(5)
     pts16 = [(int(rng.integers(0, w.nextrap)), int(rng.integers(0, w.nx))) for _ in range(16)]
     ga, fd = lsm.finite_difference_check(op, torch.zeros_like(m_true), d_obs, pts16, h=1.0)
@@ -308,8 +309,11 @@ def lsm_leg(dev, iters, scale=1.0):
                                       "source": "checkpoint pass inside the call"},
                         "kernel_config": op.plan.describe_demigration()},
         "migration": {"value": pts / t_mig, "unit": UNIT, "seconds": t_mig},
-        "dot_product": {"rel": [d[2] for d in dots], "rel_norms": [d[3] for d in dots],
-                        "seeds": 3, "vectors": "Gaussian d (complex) and m",
+        "dot_product": {"rel": [d[2] for d in dots_sep], "rel_norms": [d[3] for d in dots_sep],
+                        "rel_independent": [d[2] for d in dots], "rel_norms_independent": [d[3] for d in dots],
+                        "seeds": 5, "vectors": "Gaussian d (complex); m Gaussian plus sign(z) * 3 * Fd/||Fd|| "
+                                               "(projection on Fd kept >= 3 norms from orthogonality); "
+                                               "*_independent: m Gaussian",
                         "rel_def": "|<Fd,m> - <d,F*m>| / max(|<Fd,m>|, |<d,F*m>|)",
                         "rel_norms_def": "|<Fd,m> - <d,F*m>| / (||Fd|| ||m||)"},
         "fd_gradient": {"points": 16, "h": 1.0, "max_abs_err_over_max_grad": float(np.max(np.abs(ga - fd)) /
@@ -529,10 +533,10 @@ def main():
                                         wave0, shot0, shot_x0=w.shot_x0, shot_nx=w.shot_nx, trial_depths=8)
         tune_report = {"trial_depths": 8, "picked": rows[0][1],
                        "ms": {n: round(t, 3) for t, n, _ in rows}}
-        plan = migration.Plan.for_workload(w, **best)
     else:
-        plan = migration.Plan.for_workload(w, no_cluster=args.kernel == "single",
-                                           cluster_v1=args.kernel == "cluster1", variant=args.variant)
+        best = dict(no_cluster=args.kernel == "single", cluster_v1=args.kernel == "cluster1", variant=args.variant,
+                    wide=args.kernel == "wide", wide_scalar=args.kernel == "wide-scalar")
+    plan = migration.Plan.for_workload(w, **best)
     plan.set_model(om, vel, w.dk, tab)
     wave = torch.empty_like(wave0)
     shot = torch.empty_like(shot0)
@@ -641,7 +645,8 @@ def main():
             ta.record(torch.cuda.default_stream())
             check(lib().img2d_migrate_compact(w.ns, w.nextrap, w.nz, w.nx, w.nf, w.nt, w.M, w.nk, float(w.dk),
                                               ptr(w.omega), ptr(vel_h), ptr(w.table), None, ptr(x0), ptr(wn),
-                                              ptr(wave_h), ptr(shot_h), ptr(img_h), None, 0))
+                                              ptr(wave_h), ptr(shot_h), ptr(img_h), None,
+                                              migration.plan_flags(**best)))
             tb.record(torch.cuda.default_stream())
             tb.synchronize()
             return ta.elapsed_time(tb) / 1e3
@@ -651,7 +656,8 @@ def main():
         h2d = w.wave.nbytes + w.shot.nbytes + w.omega.nbytes + w.nextrap * w.nx * 8 + w.table.nbytes
         d2h = w.wave.nbytes + w.shot.nbytes + w.nextrap * w.nx * 4
         extra["e2e"] = {"value": pts_rank / float(np.median(secs)), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
-                        "d2h_bytes_per_step": int(d2h), "api": "img2d_migrate_compact (host buffers)",
+                        "d2h_bytes_per_step": int(d2h), "calls": len(secs),
+                        "api": "img2d_migrate_compact (host buffers, flags of the timed kernel configuration)",
                         "n_gpus": 1}
 
     # naive one-launch-per-(shot, w, z) form on a sample of the same workload

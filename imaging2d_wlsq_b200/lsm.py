@@ -179,12 +179,18 @@ def _sync(op):
         torch.cuda.synchronize(op.device)
 
 
-def dot_product_test(op, seed=0, data=None, refl=None):
+def dot_product_test(op, seed=0, data=None, refl=None, separation=0.0):
     """<F d, m> against Re sum d conj(F* m) for seeded Gaussian d and m.  Returns
     (lhs, rhs, rel, rel_norms) with rel = |lhs - rhs| / max(|lhs|, |rhs|) and
-    rel_norms = |lhs - rhs| / (||F d|| ||m||).  Independent random vectors make lhs a sum of
-    terms of both signs, so rel grows as lhs happens to cancel; rel_norms is the same difference on
-    the Cauchy-Schwarz scale, where a wrong adjoint shows up near 1/sqrt(size of the image)."""
+    rel_norms = |lhs - rhs| / (||F d|| ||m||).
+
+    For independent Gaussian vectors lhs = ||F d|| z with z ~ N(0, 1) the normalised projection of m
+    on F d, while the FP32 rounding of F and F* contributes |lhs - rhs| ~ eps ||F d|| with eps a
+    few 1e-7; so rel ~ eps / |z| is ill-conditioned for seeds where m is nearly orthogonal to F d.
+    separation > 0 adds sign(z) * separation * F d / ||F d|| to the Gaussian m (a vector of norm
+    `separation`, against ||m|| ~ sqrt(image size)), which makes |z| >= separation for every seed
+    while m stays a Gaussian vector to within that tiny component; rel then measures eps.  A wrong
+    tap, row or depth order gives rel ~ 1e-3 either way."""
     import torch
     g = torch.Generator(device=op.device).manual_seed(seed)
     if data is None:
@@ -192,6 +198,10 @@ def dot_product_test(op, seed=0, data=None, refl=None):
     if refl is None:
         refl = torch.randn((op.nextrap, op.nx), dtype=torch.float32, device=op.device, generator=g)
     img = op.migrate(data)
+    if separation > 0.0:
+        nimg = np.sqrt(op.image_dot(img, img))
+        sgn = 1.0 if op.image_dot(img, refl) >= 0.0 else -1.0
+        refl = (refl.double() + (sgn * separation / nimg) * img.double()).float()
     lhs = op.image_dot(img, refl)
     rhs = op.data_dot(data, op.demigrate(refl))
     scale = np.sqrt(op.image_dot(img, img) * op.image_dot(refl, refl))

@@ -52,6 +52,16 @@ def migrate_workload(w, two_tables=False, table_back=None, image_shots=False, ge
     return img, imgs, wave, shot
 
 
+def plan_flags(two_tables=False, generic=False, no_cluster=False, cluster_v1=False, variant=0, table="fp32",
+               demig_ring=True, wide=False, wide_scalar=False):
+    """The C ABI `flags` word of a kernel configuration given as Plan keyword arguments."""
+    return (_lib.FLAG_TWO_TABLES if two_tables else 0) | (_lib.FLAG_GENERIC if generic else 0) | \
+        (_lib.FLAG_NO_CLUSTER if no_cluster else 0) | (_lib.FLAG_CLUSTER_V1 if cluster_v1 else 0) | \
+        (int(variant) << _lib.FLAG_VARIANT_SHIFT) | \
+        {"fp32": 0, "fp16": _lib.FLAG_TABLE_FP16, "bf16": _lib.FLAG_TABLE_BF16}[table] | \
+        (0 if demig_ring else _lib.FLAG_DEMIG_NO_RING) | _wide_flags(wide, wide_scalar)
+
+
 def _wide_flags(wide, wide_scalar):
     """Flags of the wide cluster kernel (8 slots x 1024 positions per CTA): packed FMAs by default,
     scalar FMAs with wide_scalar."""
@@ -87,11 +97,7 @@ class Plan:
             ns, nextrap, nz, nx, nf, nt, M, nk
         x0 = None if shot_x0 is None else np.ascontiguousarray(shot_x0, dtype=np.int32)
         wn = None if shot_nx is None else np.ascontiguousarray(shot_nx, dtype=np.int32)
-        flags = (_lib.FLAG_TWO_TABLES if two_tables else 0) | (_lib.FLAG_GENERIC if generic else 0) | \
-            (_lib.FLAG_NO_CLUSTER if no_cluster else 0) | (_lib.FLAG_CLUSTER_V1 if cluster_v1 else 0) | \
-            (int(variant) << _lib.FLAG_VARIANT_SHIFT) | \
-            {"fp32": 0, "fp16": _lib.FLAG_TABLE_FP16, "bf16": _lib.FLAG_TABLE_BF16}[table] | \
-            (0 if demig_ring else _lib.FLAG_DEMIG_NO_RING) | _wide_flags(wide, wide_scalar)
+        flags = plan_flags(two_tables, generic, no_cluster, cluster_v1, variant, table, demig_ring, wide, wide_scalar)
         h = ctypes.c_void_p()
         check(lib().img2d_plan_create(ctypes.byref(h), ns, nextrap, nz, nx, nf, nt, M, nk, ptr(x0), ptr(wn), flags))
         self._h = h

@@ -4,9 +4,11 @@ test_oracle_adjoint.py).
 
 Tolerances: demigrated data within 1e-5 relative L2 of the FP64 oracle (the FP32 bar of the
 migration); dot-product test <F d, m> = Re sum d conj(F* m): the classic ratio
-|<F d, m> - <d, F* m>| / |<F d, m>| within 1e-6 on five seeds per case (the FP64 oracle pair passes
-at 1e-11), and the same difference within 1e-6 of ||F d|| ||m||; finite differences of the
-quadratic misfit within 1e-3 relative.
+|<F d, m> - <d, F* m>| / |<F d, m>| within 1e-6 on five seeds per case for Gaussian m kept at least
+3 norms of F d-projection away from orthogonality (for independent Gaussian vectors the ratio is
+the FP32 error, a few 1e-7, divided by |z|, z ~ N(0, 1), and is only held to 2e-5), the same
+difference within 1e-7 of ||F d|| ||m|| (the FP64 oracle pair passes at 1e-11); finite differences
+of the quadratic misfit within 1e-3 relative.
 """
 import numpy as np
 import pytest
@@ -95,28 +97,33 @@ def test_demigration_rejects_bad_arguments():
 def test_dot_product(case):
     w = CASES[case]()
     op = _op(w)
-    rels = []
+    sep, ind = [], []
     for seed in range(5):
+        # m with |projection on F d| >= 3 (lsm.dot_product_test): the classic ratio measures the FP32 error
+        lhs, rhs, rel, rel_norms = lsm.dot_product_test(op, seed=seed, separation=3.0)
+        sep.append(rel)
+        assert rel <= 1e-6 and rel_norms <= 1e-7, (seed, lhs, rhs, rel, rel_norms)
+        # independent Gaussian m: the same FP32 error over |z|, z ~ N(0, 1)
         lhs, rhs, rel, rel_norms = lsm.dot_product_test(op, seed=seed)
-        rels.append(rel)
-        assert rel_norms <= 1e-6 and rel <= 1e-6, (seed, lhs, rhs, rel, rel_norms)
-    print(f"\ndot product {case}: rel {[f'{r:.2e}' for r in rels]}")
+        ind.append(rel)
+        assert rel_norms <= 1e-7 and rel <= 2e-5, (seed, lhs, rhs, rel, rel_norms)
+    print(f"\ndot product {case}: separated {[f'{r:.2e}' for r in sep]}, independent {[f'{r:.2e}' for r in ind]}")
     op.plan.close()
 
 
-def test_dot_product_lsm_geometry():
-    """The least-squares configuration's geometry (nx=1024, dx=dz=10 m, smooth random velocity,
-    31 taps, nk=2000, 2-40 Hz, full-aperture shots) at a reduced size: 100 depth steps, 32
-    frequencies, 16 shots.  The classic ratio |<F d, m> - <d, F* m>| / |<F d, m>| must stay within
-    1e-6 on five seeds."""
-    w = synthetic.lsm(nz=100, nf=32, ns=16)
+def test_dot_product_lsm_configuration():
+    """The least-squares configuration in full (nz=500, nx=1024, nf=256 over 2-40 Hz, 31 taps,
+    nk=2000, 64 full-aperture shots): the classic ratio |<F d, m> - <d, F* m>| / |<F d, m>| within
+    1e-6 on five seeds, for Gaussian d and Gaussian m separated from orthogonality to F d
+    (lsm.dot_product_test, separation 3)."""
+    w = synthetic.lsm()
     op = _op(w)
     rels = []
     for seed in range(5):
-        lhs, rhs, rel, rel_norms = lsm.dot_product_test(op, seed=seed)
+        lhs, rhs, rel, rel_norms = lsm.dot_product_test(op, seed=seed, separation=3.0)
         rels.append(rel)
         assert rel <= 1e-6, (seed, lhs, rhs, rel, rel_norms)
-    print(f"\ndot product lsm geometry (nz=100, nf=32, ns=16): rel {[f'{r:.2e}' for r in rels]}")
+    print(f"\ndot product lsm configuration: separated {[f'{r:.2e}' for r in rels]}")
     op.plan.close()
 
 
@@ -241,8 +248,8 @@ def test_cluster_demigration_matches_oracle_and_single_cta(case, slab):
     for mode in ("keep", "reuse"):
         assert np.array_equal(data[mode], data["recompute"]), mode
     assert np.array_equal(data["recompute"], d1.cpu().numpy())
-    lhs, rhs, rel, rel_norms = lsm.dot_product_test(op, seed=2)
-    assert rel_norms <= 1e-6 and rel <= 2e-5, (lhs, rhs, rel, rel_norms)
+    lhs, rhs, rel, rel_norms = lsm.dot_product_test(op, seed=2, separation=3.0)
+    assert rel_norms <= 1e-7 and rel <= 1e-6, (lhs, rhs, rel, rel_norms)
     op.plan.close()
     single.plan.close()
 
