@@ -35,10 +35,14 @@ METRIC = "extrapolated pts/s (shot*w*z*x), batched vs plain on 1 GPU; rel-L2 err
 UNIT = "pts/s"
 
 
-# ncu (dram__bytes_read.sum + dram__bytes_write.sum, one pass) of one full batched_uneven launch,
-# per cluster-kernel variant index: the staged variant 98.07 + 78.56 GB, the ring (default)
-# 98.29 + 76.61 GB
-PROFILED_TRAFFIC_BYTES = {10: 176.63e9, 11: 174.90e9}
+# DRAM and L2 traffic per extrapolated point of the migration kernels, measured by one ncu capture of
+# the small case of the batched_uneven workload (nz=60, nf=64: 9.68e8 points per launch):
+# dram = (dram__bytes_read.sum + dram__bytes_write.sum) / points, l2 = lts__t_sectors.sum * 32 / points.
+# Keyed by (kernel, variant) of describe(); the bench scales them by the points of its launch.
+TRAFFIC_PER_POINT = {
+    ("migrate_wide", 1): {"dram": 2.41, "l2": 86.0, "capture": "migrate_wide_kernel<1>, nz=60 nf=64"},
+    ("migrate_cluster2", 11): {"dram": 0.980, "l2": 45.8, "capture": "migrate_cluster2_kernel ring variant, nz=60 nf=64"},
+}
 
 
 def parse_args():
@@ -593,34 +597,39 @@ def main():
                 "per_point": f"{flops_pt} flop (16L+4, L={w.L})",
                 "peak_source": "FP32 FMA probe kernel timed in this run (img2d_measure_fp32_peak); "
                                "MEASURED_PEAKS.json has no FP32 CUDA-core peak"}
-        ach_b = pts_rank * bytes_pt / k_s / 1e9
-        roof_hbm = {"bound": "hbm", "achieved": ach_b, "peak": hbm, "unit": "GB/s", "frac": ach_b / hbm,
-                    "per_point": f"{bytes_pt} B (8L operator bytes, no cross-shot reuse credit)",
-                    "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({hbm_src})",
-                    "note": "operator rows are served from L2/L1 and reused across the shots of a CTA, "
-                            "so this algorithmic-bytes ratio exceeds 1; the FP32 roofline binds"}
-        # DRAM bytes of one launch of the default kernel on the full batched_uneven workload, from one
-        # ncu capture (dram__bytes_read.sum + dram__bytes_write.sum, single pass); other shapes: null
-        if (w.name == "batched_uneven" and args.scale == 1.0 and not (args.nz or args.nf or args.taps)
-                and describe.get("kernel") == "migrate_cluster2"
-                and describe.get("variant") in PROFILED_TRAFFIC_BYTES and world == 1):
-            traffic = PROFILED_TRAFFIC_BYTES[describe["variant"]]
-            roof["traffic"] = traffic
-            roof["traffic_unit"] = "bytes per launch"
-            roof["traffic_source"] = "profiles/migrate_cluster2_kernel_batched_uneven.md"
-            roof_hbm["traffic_gbs"] = traffic / k_s / 1e9
+        # per-point figures of the captured configuration only (batched_uneven geometry, 35 taps)
+        tp = TRAFFIC_PER_POINT.get((describe.get("kernel"), describe.get("variant"))) \
+            if (w.name == "batched_uneven" and w.L == 35) else None
         l2 = migration.l2_read_bandwidth_gbs()
-        roof_l2 = {"bound": "l2", "achieved": ach_b, "peak": l2, "unit": "GB/s", "frac": ach_b / l2,
-                   "per_point": f"{bytes_pt} B (8L operator bytes gathered per point)",
+        ach_alg = pts_rank * bytes_pt / k_s / 1e9
+        roof_hbm = {"bound": "hbm", "achieved": None, "peak": hbm, "unit": "GB/s", "frac": None,
+                    "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({hbm_src})",
+                    "algorithmic_gbs": ach_alg,
+                    "algorithmic_per_point": f"{bytes_pt} B (8L operator bytes, no cross-shot reuse credit); "
+                                             "the rows are reused by the slots of an item from shared memory, "
+                                             "so this rate is not a DRAM stream"}
+        roof_l2 = {"bound": "l2", "achieved": None, "peak": l2, "unit": "GB/s", "frac": None,
                    "peak_source": "L2 read probe timed in this run (img2d_measure_l2_bandwidth); "
-                                  "MEASURED_PEAKS.json has no L2 figure",
-                   "note": "the compact table (1.1 MB) is L2-resident; the rows a CTA reuses across its "
-                           "16 lane slots are served from L1, so L2 carries a fraction of these bytes"}
+                                  "MEASURED_PEAKS.json has no L2 figure"}
+        if tp:
+            # measured bytes per point (small-case ncu capture) x the points of this launch
+            traffic = tp["dram"] * pts_rank
+            roof["traffic"] = traffic
+            roof["traffic_unit"] = "DRAM bytes per launch"
+            roof["traffic_source"] = (f"{tp['dram']} B/point from ncu of the small case ({tp['capture']}), "
+                                      "scaled by this launch's points")
+            roof_hbm.update(achieved=traffic / k_s / 1e9, frac=traffic / k_s / 1e9 / hbm,
+                            per_point=f"{tp['dram']} B measured DRAM traffic (scaled from the small case)")
+            l2b = tp["l2"] * pts_rank
+            roof_l2.update(achieved=l2b / k_s / 1e9, frac=l2b / k_s / 1e9 / l2,
+                           per_point=f"{tp['l2']} B measured L2 traffic (lts__t_sectors x 32, scaled from the "
+                                     "small case)")
         extra["roofline"] = roof
         extra["roofline_hbm"] = roof_hbm
         extra["roofline_l2"] = roof_l2
-        extra["binding"] = ("fp32: FP32 FMA work is the largest fraction of its measured peak; the operator "
-                            "stream is served by L1/L2 reuse, DRAM traffic is the image partials")
+        extra["binding"] = ("fp32: FP32 FMA work is the largest fraction of its measured peak; L2 and DRAM "
+                            "carry measured traffic far below their peaks (operator rows reused from shared "
+                            "memory; DRAM traffic is mostly the per-CTA Kahan partial-image rows)")
         extra["kernel_config"] = describe
         if tune_report:
             extra["autotune"] = tune_report

@@ -662,8 +662,12 @@ static int build_plan(img2d_plan *p, int ns, int nextrap, int nz, int nx, int nf
     // Wide cluster kernel (8 slots x 1024 positions per CTA, clusters of half the size): on request
     if (!p->cluster && !tab16 && mode == OP_CONJ && (flags & IMG2D_FLAG_WIDE) &&
         !(flags & (IMG2D_FLAG_GENERIC | IMG2D_FLAG_NO_CLUSTER)) && p->L >= 7) {
-        const KernelFn wf = (flags & IMG2D_FLAG_WIDE_SCALAR) ? migrate_wide_kernel<0> : migrate_wide_kernel<1>;
-        const size_t smemw = wide_smem_bytes(M);
+        // with the step-ahead stage where its 12 KB fit (operators up to 49 taps)
+        const bool stage = wide_stage_smem_bytes(M) + static_reserve <= (size_t)smem_optin;
+        const KernelFn wf = (flags & IMG2D_FLAG_WIDE_SCALAR)
+                                ? (stage ? migrate_wide_kernel<0, true> : migrate_wide_kernel<0, false>)
+                                : (stage ? migrate_wide_kernel<1, true> : migrate_wide_kernel<1, false>);
+        const size_t smemw = stage ? wide_stage_smem_bytes(M) : wide_smem_bytes(M);
         if (smemw + static_reserve <= (size_t)smem_optin) {
             const int widest = make_groups(WideShape::G);
             const int K = (widest + WideShape::PC - 1) / WideShape::PC;
@@ -675,7 +679,7 @@ static int build_plan(img2d_plan *p, int ns, int nextrap, int nz, int nx, int nf
                 p->smem = smemw;
                 p->max_w = widest;
                 p->block = WideShape::NW * 32;
-                p->variant = (flags & IMG2D_FLAG_WIDE_SCALAR) ? 0 : 1;
+                p->variant = ((flags & IMG2D_FLAG_WIDE_SCALAR) ? 0 : 1) + (stage ? 2 : 0);
                 p->kname = "migrate_wide";
             }
         }

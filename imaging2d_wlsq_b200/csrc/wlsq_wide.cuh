@@ -27,14 +27,15 @@
 // Operator taps reach the tap loop through the per-lane-group shared-memory ring of the cluster2
 // ring variant: lane q owns outputs q and q+4 of its group's block and copies their tap pairs with
 // 16-byte cp.async three tap-loop iterations before they are read.  The next depth step's operator
-// indices and this step's Kahan partial-image values of those two positions are loaded at the
-// start of the step and arrive during the tap loop.
+// indices and this step's Kahan partial-image values of those two positions reach the thread
+// through a per-thread shared-memory stage filled by cp.async a step ahead (STAGE, where the
+// shared memory allows), or are loaded into registers at the start of the step.
 //
 // Per depth step: tap loop into registers; aperture mask; edge outputs pushed into the neighbour's
-// halo staging (distributed shared memory, double-buffered by step parity); __syncthreads;
-// in-place write; split cluster barrier with the imaging (Re(S conj R), shuffle over the group's 4
-// lanes, Kahan update of the CTA's private partial row) between its halves; halo copy;
-// __syncthreads.
+// halo staging (distributed shared memory, double-buffered by step parity); cluster barrier arrive
+// (release of the pushes); the next step's first tap pairs copied; __syncthreads;
+// in-place write; imaging (Re(S conj R), shuffle over the group's 4 lanes, Kahan update of the
+// CTA's private partial row); cluster barrier wait; halo copy; __syncthreads.
 #pragma once
 #include "wlsq_cluster2.cuh"
 
@@ -58,6 +59,16 @@ __host__ __device__ inline size_t wide_smem_bytes(int M)
     const int mp = cluster2_mp(M);
     return (size_t)((WideShape::PC + 2 * mp) + 4 * mp) * WideShape::G * 16 +
            (size_t)WideShape::NG * WideShape::RING * 16;
+}
+
+// Step-ahead stage (STAGE): per thread 6 words after the rings, the aligned index words holding the
+// next depth step's operator indices of its two outputs and this step's Kahan partial and
+// compensation values of its two positions.  Each thread reads only its own words, then refills
+// them with cp.async for a later step.
+constexpr int kWideStageWords = 6;
+__host__ __device__ inline size_t wide_stage_smem_bytes(int M)
+{
+    return wide_smem_bytes(M) + (size_t)WideShape::NW * 32 * kWideStageWords * 4;
 }
 
 // float4 column of half h (0 = S, 1 = conj R) of lane q in row pos
@@ -89,7 +100,10 @@ __device__ __forceinline__ void wide_mac(float (&c)[8], float fr, float fi, cons
     }
 }
 
-template <int ARITH>
+// STAGE: the next step's operator indices and this step's Kahan values reach the thread through its
+// shared-memory stage words, copied by cp.async one step ahead (no register holds a pending load
+// across the tap loop); otherwise they are loaded into registers at the start of the step.
+template <int ARITH, bool STAGE>
 __global__ void __launch_bounds__(WideShape::NW * 32, 1) migrate_wide_kernel(MigrateArgs a)
 {
     using S = WideShape;
@@ -112,6 +126,9 @@ __global__ void __launch_bounds__(WideShape::NW * 32, 1) migrate_wide_kernel(Mig
     const bool push_right = crank + 1 < csize && b * X + X > PC - MP;
     // this lane group's ring, [output][slot] float4 plus one pad, after the halo staging
     float4 *const ringb = smem + (size_t)(NEXT + 4 * MP) * G + (size_t)b * S::RING;
+    // STAGE: this thread's words [idx word of output q, of q+4, s0, c0, s1, c1]
+    unsigned *const sst = reinterpret_cast<unsigned *>(smem + (size_t)(NEXT + 4 * MP) * G + (size_t)S::NG * S::RING) +
+                          (size_t)threadIdx.x * kWideStageWords;
     const int npairs = (L + 1) >> 1;
     const unsigned rank0_item = map_rank(&s_item, 0);
     const int row_bytes = a.tab_stride * 8;
@@ -181,6 +198,25 @@ __global__ void __launch_bounds__(WideShape::NW * 32, 1) migrate_wide_kernel(Mig
         unsigned roff0 = (unsigned)idx_j[xq0] * (unsigned)row_bytes;
         unsigned roff1 = (unsigned)idx_j[xq1] * (unsigned)row_bytes;
         unsigned nidx01 = 0;  // next step's row indices of outputs q (low half) and q+4 (high half)
+        // STAGE: copies of the aligned index words of step ls (outputs q and q+4) and of the Kahan
+        // values of step lk (positions q and q+4) into this thread's stage words
+        auto stage_idx = [&](int ls) {
+            const uint16_t *ip = idx_j + (long long)ls * a.idx_lstride;
+            cp_async4(sst + 0, ip + (xq0 & ~1));
+            cp_async4(sst + 1, ip + (xq1 & ~1));
+        };
+        const long long prow0 = (long long)blockIdx.x * a.nextrap * a.nx + xg + q;  // partial element of step 0
+        auto stage_kahan = [&](int lk) {
+            const long long e = prow0 + (long long)lk * a.nx;
+            if (img0) {
+                cp_async4(sst + 2, a.partial + e);
+                cp_async4(sst + 3, a.comp + e);
+            }
+            if (img1) {
+                cp_async4(sst + 4, a.partial + e + Q);
+                cp_async4(sst + 5, a.comp + e + Q);
+            }
+        };
         // branch-free: a pair outside the row becomes a zero-filled copy of nothing (never read)
         auto ring_copy = [&](int u) {
             const char *tabb = reinterpret_cast<const char *>(a.tabF);
@@ -191,30 +227,41 @@ __global__ void __launch_bounds__(WideShape::NW * 32, 1) migrate_wide_kernel(Mig
             cp_async16_zfill(ringb + (q + Q) * kRingSlots + sl, tabb + roff1 + (ok1 ? pr1 : 0) * 16, ok1 ? 16u : 0u);
         };
         for (int u = -(X / 2); u < 0; ++u) ring_copy(u);
+        if (STAGE) {
+            if (a.nextrap > 1) stage_idx(1);
+            stage_kahan(0);
+        }
         cp_async_commit();
         const int srow0 = b * X + MP - M;  // row of input t = 0
-        const long long prow0 = (long long)blockIdx.x * a.nextrap * a.nx + xg + q;  // partial element of step 0
 
         for (int l = 0; l < a.nextrap; ++l) {
             const int par = l & 1;
             // this step's prologue pairs (copied at the end of the previous step) for the group
             cp_async_wait_all();
             __syncwarp();  // control flow is warp-uniform here
-            // this step's Kahan values and the next step's operator indices: the loads are issued
-            // here and complete during the tap loop
             const long long pe = prow0 + (long long)l * a.nx;
             float cur_s0 = 0.f, cur_c0 = 0.f, cur_s1 = 0.f, cur_c1 = 0.f;
-            if (img0) {
-                cur_s0 = a.partial[pe];
-                cur_c0 = a.comp[pe];
+            if (!STAGE) {
+                // this step's Kahan values and the next step's operator indices: the loads are
+                // issued here and complete during the tap loop
+                if (img0) {
+                    cur_s0 = a.partial[pe];
+                    cur_c0 = a.comp[pe];
+                }
+                if (img1) {
+                    cur_s1 = a.partial[pe + Q];
+                    cur_c1 = a.comp[pe + Q];
+                }
+                if (l + 1 < a.nextrap) {
+                    const uint16_t *inext = idx_j + (long long)(l + 1) * a.idx_lstride;
+                    nidx01 = (unsigned)inext[xq0] | ((unsigned)inext[xq1] << 16);
+                }
             }
-            if (img1) {
-                cur_s1 = a.partial[pe + Q];
-                cur_c1 = a.comp[pe + Q];
-            }
-            if (l + 1 < a.nextrap) {
-                const uint16_t *inext = idx_j + (long long)(l + 1) * a.idx_lstride;
-                nidx01 = (unsigned)inext[xq0] | ((unsigned)inext[xq1] << 16);
+            // the partial-image rows of the next step into L2 (read at the end of this step by the
+            // stage, or at the start of the next one)
+            if (q == 0 && img0 && l + 1 < a.nextrap) {
+                asm volatile("prefetch.global.L2 [%0];" ::"l"(a.partial + pe + a.nx));
+                asm volatile("prefetch.global.L2 [%0];" ::"l"(a.comp + pe + a.nx));
             }
             float acc[X][8];
 #pragma unroll
@@ -322,14 +369,6 @@ __global__ void __launch_bounds__(WideShape::NW * 32, 1) migrate_wide_kernel(Mig
                     if (!((in_b >> jj) & 1u)) acc[jj][1] = acc[jj][3] = acc[jj][5] = acc[jj][7] = 0.f;
                 }
             }
-            // every ring slot has been read: copy the next step's prologue pairs (u < 0) now, so
-            // that they arrive during the halo exchange and the imaging
-            if (l + 1 < a.nextrap) {
-                roff0 = (nidx01 & 0xffffu) * (unsigned)row_bytes;
-                roff1 = (nidx01 >> 16) * (unsigned)row_bytes;
-                for (int u = -(X / 2); u < 0; ++u) ring_copy(u);
-            }
-            cp_async_commit();
             // halos of step l+1 into the neighbours' staging (parity par^1): left neighbour's right
             // halo rows are its ext rows PC + MP + x, right neighbour's left halo rows its rows x
             if (push_left) {
@@ -357,6 +396,28 @@ __global__ void __launch_bounds__(WideShape::NW * 32, 1) migrate_wide_kernel(Mig
                     }
                 }
             }
+            // The neighbours read only their halo staging (the pushes above), never this CTA's ext[]:
+            // arrive now, so the barrier's release covers the pushes but not the in-place writes.
+            // The staging of parity par^1 is rewritten (step l+2) only after this CTA's arrival of
+            // step l+1, which follows its copy of that staging at the end of this step.
+            cluster_arrive();
+            // every ring slot has been read: copy the next step's prologue pairs (u < 0) now, so
+            // that they arrive during the halo exchange and the imaging
+            if (l + 1 < a.nextrap) {
+                if (STAGE) {
+                    const unsigned w0 = sst[0], w1 = sst[1];
+                    roff0 = ((w0 >> (16 * (xq0 & 1))) & 0xffffu) * (unsigned)row_bytes;
+                    roff1 = ((w1 >> (16 * (xq1 & 1))) & 0xffffu) * (unsigned)row_bytes;
+                } else {
+                    roff0 = (nidx01 & 0xffffu) * (unsigned)row_bytes;
+                    roff1 = (nidx01 >> 16) * (unsigned)row_bytes;
+                }
+                for (int u = -(X / 2); u < 0; ++u) ring_copy(u);
+                // the words just read are refilled for step l + 2 (their reads are complete: the
+                // copies above used them)
+                if (STAGE && l + 2 < a.nextrap) stage_idx(l + 2);
+            }
+            cp_async_commit();
             __syncthreads();  // every read of step l's values in ext[] is done
 #pragma unroll
             for (int jj = 0; jj < X; ++jj) {
@@ -365,7 +426,6 @@ __global__ void __launch_bounds__(WideShape::NW * 32, 1) migrate_wide_kernel(Mig
                 dst[wide_col(prow, q, 0)] = make_float4(acc[jj][0], acc[jj][1], acc[jj][2], acc[jj][3]);
                 dst[wide_col(prow, q, 1)] = make_float4(acc[jj][4], acc[jj][5], acc[jj][6], acc[jj][7]);
             }
-            cluster_arrive();
             float img_q0 = 0.f, img_q1 = 0.f;  // stacked image values of the lane's two positions
 #pragma unroll
             for (int jj = 0; jj < X; ++jj) {
@@ -389,6 +449,12 @@ __global__ void __launch_bounds__(WideShape::NW * 32, 1) migrate_wide_kernel(Mig
                 if (jj == q + Q) img_q1 = img;
             }
             // Kahan update (the operations of kahan_add) on the values loaded at the step's start
+            if (STAGE) {
+                cur_s0 = __uint_as_float(sst[2]);
+                cur_c0 = __uint_as_float(sst[3]);
+                cur_s1 = __uint_as_float(sst[4]);
+                cur_c1 = __uint_as_float(sst[5]);
+            }
             if (img0) {
                 const float y = img_q0 - cur_c0;
                 const float t = cur_s0 + y;
@@ -400,6 +466,11 @@ __global__ void __launch_bounds__(WideShape::NW * 32, 1) migrate_wide_kernel(Mig
                 const float t = cur_s1 + y;
                 a.partial[pe + Q] = t;
                 a.comp[pe + Q] = (t - cur_s1) - y;
+            }
+            if (STAGE) {
+                // refill the Kahan words for the next step (waited for at its start)
+                if (l + 1 < a.nextrap) stage_kahan(l + 1);
+                cp_async_commit();
             }
             cluster_wait();
             const float4 *hs = stg + (size_t)((par ^ 1) * 2) * MP * G;
