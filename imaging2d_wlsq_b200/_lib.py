@@ -31,6 +31,7 @@ FLAG_TABLE_BF16 = 32
 FLAG_DEMIG_NO_RING = 64
 FLAG_WIDE = 128
 FLAG_WIDE_SCALAR = 1 << 16
+FLAG_CLUSTER2 = 1 << 17
 NOALLOC_SCRATCH_BYTES = 64 << 20
 
 ERROR_NAMES = {1: "EINVAL", 2: "ENOMEM", 3: "ECUDA", 4: "ENODEV"}

@@ -653,36 +653,56 @@ static int build_plan(img2d_plan *p, int ns, int nextrap, int nz, int nx, int nf
         p->kname = "migrate_cluster2";
         return true;
     };
-    if (cluster_ok && !(flags & (IMG2D_FLAG_CLUSTER_V1 | IMG2D_FLAG_WIDE)) && p->L >= 7) {
-        // the default ring variant needs 33 KB more shared memory than the staged one: long
-        // operators or very wide windows fall back to the staged variant
-        if (!try_cluster2(cv, vsel) && !explicit_variant && !tab16 && vsel != kCluster2Staged)
-            try_cluster2(kCluster2[kCluster2Staged], kCluster2Staged);
-    }
-    // Wide cluster kernel (8 slots x 1024 positions per CTA, clusters of half the size): on request
-    if (!p->cluster && !tab16 && mode == OP_CONJ && (flags & IMG2D_FLAG_WIDE) &&
-        !(flags & (IMG2D_FLAG_GENERIC | IMG2D_FLAG_NO_CLUSTER)) && p->L >= 7) {
+    // Wide cluster kernel (8 slots x 1024 positions per CTA, clusters of half the size, packed FMAs).
+    // It is the default where the cluster2 kernel's clusters would leave SMs idle (clusters of 4 fit
+    // 33 times on 148 SMs), and on request (IMG2D_FLAG_WIDE / _WIDE_SCALAR).
+    auto try_wide = [&]() {
         // with the step-ahead stage where its 12 KB fit (operators up to 49 taps)
         const bool stage = wide_stage_smem_bytes(M) + static_reserve <= (size_t)smem_optin;
         const KernelFn wf = (flags & IMG2D_FLAG_WIDE_SCALAR)
                                 ? (stage ? migrate_wide_kernel<0, true> : migrate_wide_kernel<0, false>)
                                 : (stage ? migrate_wide_kernel<1, true> : migrate_wide_kernel<1, false>);
         const size_t smemw = stage ? wide_stage_smem_bytes(M) : wide_smem_bytes(M);
-        if (smemw + static_reserve <= (size_t)smem_optin) {
-            const int widest = make_groups(WideShape::G);
-            const int K = (widest + WideShape::PC - 1) / WideShape::PC;
-            if (K <= 8 || (K <= kMaxCluster && clusters_that_fit((const void *)wf, K, WideShape::NW * 32, smemw) > 0)) {
-                p->cluster = K;
-                p->G = WideShape::G;
-                p->fixed = true;
-                p->fn = wf;
-                p->smem = smemw;
-                p->max_w = widest;
-                p->block = WideShape::NW * 32;
-                p->variant = ((flags & IMG2D_FLAG_WIDE_SCALAR) ? 0 : 1) + (stage ? 2 : 0);
-                p->kname = "migrate_wide";
-            }
-        }
+        if (smemw + static_reserve > (size_t)smem_optin) return false;
+        const int widest = make_groups(WideShape::G);
+        const int K = (widest + WideShape::PC - 1) / WideShape::PC;
+        if (!(K <= 8 || (K <= kMaxCluster && clusters_that_fit((const void *)wf, K, WideShape::NW * 32, smemw) > 0)))
+            return false;
+        p->cluster = K;
+        p->G = WideShape::G;
+        p->fixed = true;
+        p->fn = wf;
+        p->smem = smemw;
+        p->max_w = widest;
+        p->block = WideShape::NW * 32;
+        p->variant = ((flags & IMG2D_FLAG_WIDE_SCALAR) ? 0 : 1) + (stage ? 2 : 0);
+        p->kname = "migrate_wide";
+        return true;
+    };
+    const bool wide_requested = (flags & (IMG2D_FLAG_WIDE | IMG2D_FLAG_WIDE_SCALAR)) != 0;
+    const bool wide_ok = mode == OP_CONJ && !tab16 && p->L >= 7 &&
+                         !(flags & (IMG2D_FLAG_GENERIC | IMG2D_FLAG_NO_CLUSTER | IMG2D_FLAG_CLUSTER_V1 |
+                                    IMG2D_FLAG_CLUSTER2)) &&
+                         !explicit_variant && (wide_requested || p->n_slots >= 6);
+    bool want_wide = wide_ok && wide_requested;
+    if (wide_ok && !wide_requested) {
+        // default choice: SMs the cluster2 kernel would keep busy on this geometry
+        const int pc2 = cv.nw * 32;
+        const size_t smem2 = cluster2_smem_bytes(M, pc2) + (cv.stage ? cluster2_stage_bytes(pc2) : 0) +
+                             (cv.ring ? cluster2_ring_bytes(pc2) : 0);
+        const int K2 = (make_groups(16) + pc2 - 1) / pc2;
+        const int busy = smem2 + static_reserve <= (size_t)smem_optin && K2 <= kMaxCluster
+                             ? clusters_that_fit((const void *)cv.fn, K2, pc2, smem2) * K2
+                             : 0;
+        want_wide = p->n_slots < 12 || busy < nsm * 96 / 100;
+    }
+    if (want_wide) try_wide();
+    if (!p->cluster && cluster_ok && !(flags & (IMG2D_FLAG_CLUSTER_V1 | IMG2D_FLAG_WIDE | IMG2D_FLAG_WIDE_SCALAR)) &&
+        p->L >= 7) {
+        // the default ring variant needs 33 KB more shared memory than the staged one: long
+        // operators or very wide windows fall back to the staged variant
+        if (!try_cluster2(cv, vsel) && !explicit_variant && !tab16 && vsel != kCluster2Staged)
+            try_cluster2(kCluster2[kCluster2Staged], kCluster2Staged);
     }
     if (tab16 && !p->cluster)
         return fail(IMG2D_EINVAL, "16-bit operator tables need the cluster kernel (>= 12 lane slots, 2M+1 >= 7, "

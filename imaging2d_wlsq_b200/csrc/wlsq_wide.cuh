@@ -121,9 +121,6 @@ __global__ void __launch_bounds__(WideShape::NW * 32, 1) migrate_wide_kernel(Mig
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int p = lane / Q, q = lane % Q;
     const int b = warp * P + p;  // this lane group's block: local positions [b*X, b*X+X)
-    const int c0 = (int)crank * PC;
-    const bool push_left = crank > 0 && b * X < MP;
-    const bool push_right = crank + 1 < csize && b * X + X > PC - MP;
     // this lane group's ring, [output][slot] float4 plus one pad, after the halo staging
     float4 *const ringb = smem + (size_t)(NEXT + 4 * MP) * G + (size_t)b * S::RING;
     // STAGE: this thread's words [idx word of output q, of q+4, s0, c0, s1, c1]
@@ -146,13 +143,24 @@ __global__ void __launch_bounds__(WideShape::NW * 32, 1) migrate_wide_kernel(Mig
         const int2 item = a.items[it];
         const GroupDesc grp = a.groups[item.x];
         const int j = item.y, u0 = grp.u0, W = grp.W;
+        // The item's window is split evenly over the cluster in units of 4 warps (256 positions, one
+        // warp per SM sub-partition): each CTA owns NC <= PC consecutive positions starting at c0,
+        // and warps past NC skip the step's work.  A narrow window then leaves every sub-partition
+        // one warp less to run instead of computing positions past the window (finer units would
+        // leave the busiest sub-partition as loaded as before).
+        const int NC = min(PC, (W + (int)csize * 256 - 1) / ((int)csize * 256) * 256);
+        const int c0 = (int)crank * NC;
+        const int own = max(0, min(NC, W - c0));  // window positions this CTA owns (the rest are past W)
+        const bool warp_active = warp * (P * X) < NC;
+        const bool push_left = crank > 0 && b * X < MP;
+        const bool push_right = crank + 1 < csize && b * X + X > NC - MP && b * X < NC;
 
         for (int i = threadIdx.x; i < (NEXT + 4 * MP) * G; i += blockDim.x) smem[i] = make_float4(0.f, 0.f, 0.f, 0.f);
         __syncthreads();
         for (int k = grp.seg_begin; k < grp.seg_begin + grp.nseg; ++k) {
             const int4 sg = a.segs[k];
             const int r0 = sg.z - u0;
-            const int lo = max(r0, c0 - MP), hi = min(r0 + sg.w, c0 + PC + MP);
+            const int lo = max(r0, c0 - MP), hi = min(r0 + sg.w, c0 + NC + MP);
             const cpx *ws = a.wave + a.shot_off[sg.x] + (long long)j * sg.w;
             const cpx *rs = a.shot + a.shot_off[sg.x] + (long long)j * sg.w;
             const int sq = sg.y & (Q - 1), sh = sg.y / Q;  // lane and half (x/z or y/w) of the slot
@@ -171,7 +179,7 @@ __global__ void __launch_bounds__(WideShape::NW * 32, 1) migrate_wide_kernel(Mig
         cluster_arrive();
         cluster_wait();
 
-        const bool blk_active = c0 + b * X < W;
+        const bool blk_active = b * X < own;
         unsigned in_a = 0, in_b = 0;  // bit jj: output jj of slot q (q+4) is inside a shot's aperture
         {
             const int16_t *own_a = (blk_active && q < grp.nslots)
@@ -194,7 +202,7 @@ __global__ void __launch_bounds__(WideShape::NW * 32, 1) migrate_wide_kernel(Mig
         // lane q owns outputs q and q+4 of the block: their operator rows (byte offsets into the
         // table), next-step indices and Kahan partial-image values
         const int xq0 = min(xg + q, a.nx - 1), xq1 = min(xg + q + Q, a.nx - 1);
-        const bool img0 = a.partial && c0 + b * X + q < W, img1 = a.partial && c0 + b * X + q + Q < W;
+        const bool img0 = a.partial && b * X + q < own, img1 = a.partial && b * X + q + Q < own;
         unsigned roff0 = (unsigned)idx_j[xq0] * (unsigned)row_bytes;
         unsigned roff1 = (unsigned)idx_j[xq1] * (unsigned)row_bytes;
         unsigned nidx01 = 0;  // next step's row indices of outputs q (low half) and q+4 (high half)
@@ -226,10 +234,12 @@ __global__ void __launch_bounds__(WideShape::NW * 32, 1) migrate_wide_kernel(Mig
             cp_async16_zfill(ringb + q * kRingSlots + sl, tabb + roff0 + (ok0 ? pr0 : 0) * 16, ok0 ? 16u : 0u);
             cp_async16_zfill(ringb + (q + Q) * kRingSlots + sl, tabb + roff1 + (ok1 ? pr1 : 0) * 16, ok1 ? 16u : 0u);
         };
-        for (int u = -(X / 2); u < 0; ++u) ring_copy(u);
-        if (STAGE) {
-            if (a.nextrap > 1) stage_idx(1);
-            stage_kahan(0);
+        if (warp_active) {
+            for (int u = -(X / 2); u < 0; ++u) ring_copy(u);
+            if (STAGE) {
+                if (a.nextrap > 1) stage_idx(1);
+                stage_kahan(0);
+            }
         }
         cp_async_commit();
         const int srow0 = b * X + MP - M;  // row of input t = 0
@@ -268,6 +278,7 @@ __global__ void __launch_bounds__(WideShape::NW * 32, 1) migrate_wide_kernel(Mig
             for (int jj = 0; jj < X; ++jj)
 #pragma unroll
                 for (int e = 0; e < 8; ++e) acc[jj][e] = 0.f;
+            if (warp_active) {  // warps past the CTA's share of the window skip the step's work
             float4 tp[X];
             // input t: row srow0 + t, columns wide_col(row, q, 0/1)
             auto load_in = [&](int row, float4 &va, float4 &vb) {
@@ -377,7 +388,7 @@ __global__ void __launch_bounds__(WideShape::NW * 32, 1) migrate_wide_kernel(Mig
                 for (int jj = 0; jj < X; ++jj) {
                     const int x = b * X + jj;
                     if (x < MP) {
-                        const int prow = PC + MP + x;
+                        const int prow = NC + MP + x;
                         const unsigned ra = map_rank(dst + (size_t)x * G, crank - 1);
                         st_cluster(ra + wide_col(prow, q, 0) * 16, make_float4(acc[jj][0], acc[jj][1], acc[jj][2], acc[jj][3]));
                         st_cluster(ra + wide_col(prow, q, 1) * 16, make_float4(acc[jj][4], acc[jj][5], acc[jj][6], acc[jj][7]));
@@ -388,7 +399,7 @@ __global__ void __launch_bounds__(WideShape::NW * 32, 1) migrate_wide_kernel(Mig
                 float4 *dst = stg + ((size_t)((par ^ 1) * 2 + 0) * MP) * G;
 #pragma unroll
                 for (int jj = 0; jj < X; ++jj) {
-                    const int x = b * X + jj - (PC - MP);
+                    const int x = b * X + jj - (NC - MP);
                     if (x >= 0) {
                         const unsigned ra = map_rank(dst + (size_t)x * G, crank + 1);
                         st_cluster(ra + wide_col(x, q, 0) * 16, make_float4(acc[jj][0], acc[jj][1], acc[jj][2], acc[jj][3]));
@@ -396,6 +407,7 @@ __global__ void __launch_bounds__(WideShape::NW * 32, 1) migrate_wide_kernel(Mig
                     }
                 }
             }
+            }  // warp_active
             // The neighbours read only their halo staging (the pushes above), never this CTA's ext[]:
             // arrive now, so the barrier's release covers the pushes but not the in-place writes.
             // The staging of parity par^1 is rewritten (step l+2) only after this CTA's arrival of
@@ -403,7 +415,7 @@ __global__ void __launch_bounds__(WideShape::NW * 32, 1) migrate_wide_kernel(Mig
             cluster_arrive();
             // every ring slot has been read: copy the next step's prologue pairs (u < 0) now, so
             // that they arrive during the halo exchange and the imaging
-            if (l + 1 < a.nextrap) {
+            if (warp_active && l + 1 < a.nextrap) {
                 if (STAGE) {
                     const unsigned w0 = sst[0], w1 = sst[1];
                     roff0 = ((w0 >> (16 * (xq0 & 1))) & 0xffffu) * (unsigned)row_bytes;
@@ -419,6 +431,7 @@ __global__ void __launch_bounds__(WideShape::NW * 32, 1) migrate_wide_kernel(Mig
             }
             cp_async_commit();
             __syncthreads();  // every read of step l's values in ext[] is done
+            if (warp_active) {
 #pragma unroll
             for (int jj = 0; jj < X; ++jj) {
                 const int prow = b * X + MP + jj;
@@ -426,7 +439,10 @@ __global__ void __launch_bounds__(WideShape::NW * 32, 1) migrate_wide_kernel(Mig
                 dst[wide_col(prow, q, 0)] = make_float4(acc[jj][0], acc[jj][1], acc[jj][2], acc[jj][3]);
                 dst[wide_col(prow, q, 1)] = make_float4(acc[jj][4], acc[jj][5], acc[jj][6], acc[jj][7]);
             }
-            float img_q0 = 0.f, img_q1 = 0.f;  // stacked image values of the lane's two positions
+            // Re(S conj R) of both slots per output, summed over the group's 4 lanes by a reduce-scatter:
+            // exchange across lanes q ^ 2 keeps the 4 outputs with (jj & 2) == (q & 2), exchange
+            // across q ^ 1 keeps jj = q and q + 4 (6 shuffles instead of 8 x 2)
+            float img[X];
 #pragma unroll
             for (int jj = 0; jj < X; ++jj) {
                 const float ia = acc[jj][0] * acc[jj][4] - acc[jj][2] * acc[jj][6];
@@ -442,12 +458,25 @@ __global__ void __launch_bounds__(WideShape::NW * 32, 1) migrate_wide_kernel(Mig
                         atomicAdd(a.image_shots + (long long)orow[(long long)(q + Q) * g2.owner_stride] * a.img_sstride +
                                       (long long)l * a.nx + xg + jj, ib);
                 }
-                float img = ia + ib;
-#pragma unroll
-                for (int off = 1; off < Q; off <<= 1) img += __shfl_xor_sync(0xffffffffu, img, off);
-                if (jj == q) img_q0 = img;
-                if (jj == q + Q) img_q1 = img;
+                img[jj] = ia + ib;
             }
+            const bool hi2 = (q & 2) != 0, hi1 = (q & 1) != 0;
+            float r4[4];  // outputs {0, 1, 4, 5} ^ (q & 2)
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const int base = (i & 1) | ((i & 2) << 1);
+                const float keep = hi2 ? img[base ^ 2] : img[base];
+                const float send = hi2 ? img[base] : img[base ^ 2];
+                r4[i] = keep + __shfl_xor_sync(0xffffffffu, send, 2);
+            }
+            float img_q[2];  // outputs q and q + 4
+#pragma unroll
+            for (int k = 0; k < 2; ++k) {
+                const float keep = hi1 ? r4[2 * k + 1] : r4[2 * k];
+                const float send = hi1 ? r4[2 * k] : r4[2 * k + 1];
+                img_q[k] = keep + __shfl_xor_sync(0xffffffffu, send, 1);
+            }
+            const float img_q0 = img_q[0], img_q1 = img_q[1];
             // Kahan update (the operations of kahan_add) on the values loaded at the step's start
             if (STAGE) {
                 cur_s0 = __uint_as_float(sst[2]);
@@ -467,16 +496,14 @@ __global__ void __launch_bounds__(WideShape::NW * 32, 1) migrate_wide_kernel(Mig
                 a.partial[pe + Q] = t;
                 a.comp[pe + Q] = (t - cur_s1) - y;
             }
-            if (STAGE) {
-                // refill the Kahan words for the next step (waited for at its start)
-                if (l + 1 < a.nextrap) stage_kahan(l + 1);
-                cp_async_commit();
-            }
+            if (STAGE && l + 1 < a.nextrap) stage_kahan(l + 1);  // refilled for the next step
+            }  // warp_active
+            if (STAGE) cp_async_commit();  // the Kahan words, waited for at the next step's start
             cluster_wait();
             const float4 *hs = stg + (size_t)((par ^ 1) * 2) * MP * G;
             for (int i = threadIdx.x; i < 2 * MP * G; i += blockDim.x) {
                 const int side = i / (MP * G), r = i % (MP * G);
-                ext[(side ? (PC + MP) * G : 0) + r] = hs[i];
+                ext[(side ? (NC + MP) * G : 0) + r] = hs[i];
             }
             __syncthreads();
         }
@@ -484,7 +511,7 @@ __global__ void __launch_bounds__(WideShape::NW * 32, 1) migrate_wide_kernel(Mig
             for (int k = grp.seg_begin; k < grp.seg_begin + grp.nseg; ++k) {
                 const int4 sg = a.segs[k];
                 const int r0 = sg.z - u0;
-                const int lo = max(r0, c0), hi = min(r0 + sg.w, c0 + PC);
+                const int lo = max(r0, c0), hi = min(r0 + sg.w, c0 + own);
                 cpx *ws = a.wave + a.shot_off[sg.x] + (long long)j * sg.w;
                 cpx *rs = a.shot + a.shot_off[sg.x] + (long long)j * sg.w;
                 const int sq = sg.y & (Q - 1), sh = sg.y / Q;

@@ -42,7 +42,11 @@ typedef struct {
 #define IMG2D_FLAG_TABLE_BF16 32  /* operator table stored as BF16 (re, im) pairs, arithmetic FP32 */
 #define IMG2D_FLAG_DEMIG_NO_RING 64 /* demigration: forward steps read operator pairs through L1, not the ring */
 #define IMG2D_FLAG_WIDE 128        /* wide cluster kernel: 8 slots x 1024 positions per CTA (packed FMAs) */
-#define IMG2D_FLAG_WIDE_SCALAR (1 << 16) /* with IMG2D_FLAG_WIDE: scalar instead of packed FMAs */
+#define IMG2D_FLAG_WIDE_SCALAR (1 << 16) /* the wide cluster kernel with scalar instead of packed FMAs */
+#define IMG2D_FLAG_CLUSTER2 (1 << 17)    /* 16-slot cluster kernel (512 positions per CTA) instead */
+/* Default kernel choice: the wide cluster kernel where the 16-slot kernel's clusters would leave
+ * SMs idle (or fewer than 12 lane slots), else the 16-slot cluster kernel; the single-CTA kernels
+ * for fewer than 6 lane slots, operators shorter than 7 taps or windows beyond 16 CTAs. */
 /* select variant v (1-based; 0 = default) of the second-generation cluster kernel: bits 8-15 */
 #define IMG2D_FLAG_VARIANT_SHIFT 8
 #define IMG2D_FLAG_VARIANT(v) ((v) << IMG2D_FLAG_VARIANT_SHIFT)

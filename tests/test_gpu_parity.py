@@ -225,7 +225,7 @@ def test_cluster_kernel_matches_oracle_and_single_cta(kind, nx, nz, nf, ns, v1):
         w = synthetic.plain_medium(nx=nx, nz=nz, nf=nf, ns=ns, scale=1.0)
     else:
         w = synthetic.batched_uneven(nx=nx, nz=nz, nf=nf, ns=ns, scale=1.0)
-    plan = migration.Plan.for_workload(w, cluster_v1=v1)
+    plan = migration.Plan.for_workload(w, cluster_v1=v1, cluster2=not v1)
     d = plan.describe()
     plan.close()
     if v1 and nx > 2048:
@@ -235,7 +235,7 @@ def test_cluster_kernel_matches_oracle_and_single_cta(kind, nx, nz, nf, ns, v1):
     pc = 256 if v1 else 512
     if kind == "medium":
         assert d["cluster"] >= -(-nx // pc), d
-    img, imgs, wave, shot = migration.migrate_workload(w, image_shots=True, cluster_v1=v1)
+    img, imgs, wave, shot = migration.migrate_workload(w, image_shots=True, cluster_v1=v1, cluster2=not v1)
     e = _compact_check(w, img, wave, shot)
     img1, _, wave1, _ = migration.migrate_workload(w, no_cluster=True)
     assert rel_l2(img, img1) <= 2e-6 and rel_l2(wave, wave1) <= 2e-6
@@ -290,9 +290,9 @@ def test_ring_default_matches_staged_bitwise():
     (7 taps) and the longest whose ring still fits in shared memory (81 taps)."""
     for taps in (35, 7, 81):
         w = _with_taps(synthetic.batched_uneven(nx=1500, nz=9, nf=4, ns=48, scale=1.0), taps)
-        d = migration.Plan.for_workload(w).describe()
+        d = migration.Plan.for_workload(w, cluster2=True).describe()
         assert d["kernel"] == "migrate_cluster2" and d["variant"] == 11, (taps, d)
-        img0, _, wave0, shot0 = migration.migrate_workload(w)
+        img0, _, wave0, shot0 = migration.migrate_workload(w, cluster2=True)
         img1, _, wave1, shot1 = migration.migrate_workload(w, variant=11)
         assert np.array_equal(wave0, wave1) and np.array_equal(shot0, shot1), taps
         assert rel_l2(img0, img1) <= 1e-6, taps
@@ -311,10 +311,15 @@ def test_long_operator_falls_back_to_staged_variant():
 
 def test_wide_window_non_portable_cluster():
     """A 6000-position full-aperture window needs 12 CTAs of 512 positions: a non-portable cluster
-    size (up to 16 on B200 with the kernel's opt-in)."""
+    size (up to 16 on B200 with the kernel's opt-in) for the 16-slot kernel; the default (wide)
+    kernel covers it with 6 CTAs of 1024."""
     w = synthetic.plain_medium(nx=6000, nz=4, nf=2, ns=12)
-    d = migration.Plan.for_workload(w).describe()
+    d = migration.Plan.for_workload(w, cluster2=True).describe()
     assert d["kernel"] == "migrate_cluster2" and d["cluster"] == 12, d
+    img, _, wave, shot = migration.migrate_workload(w, cluster2=True)
+    _compact_check(w, img, wave, shot)
+    d = migration.Plan.for_workload(w).describe()
+    assert d["kernel"] == "migrate_wide" and d["cluster"] == 6, d
     img, _, wave, shot = migration.migrate_workload(w)
     _compact_check(w, img, wave, shot)
 

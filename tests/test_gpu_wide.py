@@ -1,6 +1,7 @@
 """The wide cluster kernel (8 lane slots x 1024 positions per CTA, clusters of half the size of the
-cluster2 kernel's) against the FP64 oracle (relative L2 1e-5, the compact-path bar), in both its
-packed (FFMA2) and scalar FMA forms, and bit for bit against the cluster2 kernel's final wavefields
+cluster2 kernel's, each item's window split evenly over its CTAs) against the FP64 oracle
+(relative L2 1e-5, the compact-path bar), in both its packed (FFMA2) and scalar FMA forms, with
+and without the step-ahead stage, and bit for bit against the cluster2 kernel's final wavefields
 (the same FMA sequence per element)."""
 import numpy as np
 import pytest
@@ -49,8 +50,8 @@ def test_wide_matches_fp64_oracle(case, arith):
 @pytest.mark.parametrize("arith", ARITH, ids=["ffma2", "ffma"])
 def test_wide_wavefields_bitwise_equal_cluster2(arith):
     w = synthetic.batched_uneven(scale=0.1)
-    assert migration.Plan.for_workload(w).describe()["kernel"] == "migrate_cluster2"
-    _, _, wave_c, shot_c = migration.migrate_workload(w)
+    assert migration.Plan.for_workload(w, cluster2=True).describe()["kernel"] == "migrate_cluster2"
+    _, _, wave_c, shot_c = migration.migrate_workload(w, cluster2=True)
     _, _, wave_w, shot_w = migration.migrate_workload(w, **arith)
     np.testing.assert_array_equal(wave_w, wave_c)
     np.testing.assert_array_equal(shot_w, shot_c)
@@ -87,3 +88,12 @@ def test_wide_device_plan_repeat_and_rows_beyond_nextrap():
         assert np.all(got[w.nextrap:] == 5.0)
         assert rel_l2(wave.cpu().numpy(), wo) <= 1e-5
     plan.close()
+
+
+def test_default_kernel_choice():
+    """The wide kernel is the default where the 16-slot cluster kernel's clusters of 4 would leave
+    SMs idle (2048-wide windows); the 16-slot kernel where its clusters fill the GPU."""
+    w = synthetic.batched_uneven(nz=6, nf=2)
+    assert migration.Plan.for_workload(w).describe()["kernel"] == "migrate_wide"
+    w = synthetic.plain_medium(nz=6, nf=2)  # 32 full-aperture shots over 1024 positions: clusters of 2
+    assert migration.Plan.for_workload(w).describe()["kernel"] == "migrate_cluster2"
