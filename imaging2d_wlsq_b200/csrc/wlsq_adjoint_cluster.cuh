@@ -411,6 +411,11 @@ __global__ void __launch_bounds__(kDcNW * 32, 1) demigrate_cluster_kernel(Demigr
                 const bool to_save = (l == lb) && (l > 0);
                 const float4 *Sl = (l > lb) ? slabbuf + (long long)(l - 1 - lb) * pe : ckpt + (long long)c * pe;
                 const float *mrow = l > 0 ? a.refl + (long long)(l - 1) * a.nx + base : nullptr;
+                if (mrow) {
+                    // the source plane and reflectivity row the emission after the FIR reads, into L1
+                    asm volatile("prefetch.global.L1 [%0];" ::"l"(Sl + (long long)(b * X + q) * Q));
+                    if (q == 0) asm volatile("prefetch.global.L1 [%0];" ::"l"(mrow + b * X));
+                }
                 float acc[X][4];
                 fir2_transposed<X, L>(a, bufA + q, step_idx(), xm0, pb, M, acc);
 #pragma unroll
