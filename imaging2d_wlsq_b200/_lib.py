@@ -32,6 +32,7 @@ FLAG_DEMIG_NO_RING = 64
 FLAG_WIDE = 128
 FLAG_WIDE_SCALAR = 1 << 16
 FLAG_CLUSTER2 = 1 << 17
+FLAG_WIDE_BULK = 1 << 18
 NOALLOC_SCRATCH_BYTES = 64 << 20
 
 ERROR_NAMES = {1: "EINVAL", 2: "ENOMEM", 3: "ECUDA", 4: "ENODEV"}
@@ -95,6 +96,8 @@ def load():
     lib.img2d_plan_describe.argtypes = [c_void_p, c_char_p, c_int]
     lib.img2d_plan_kernel_ms.restype = c_int
     lib.img2d_plan_kernel_ms.argtypes = [c_void_p, POINTER(ctypes.c_float)]
+    lib.img2d_plan_status.restype = c_int
+    lib.img2d_plan_status.argtypes = [c_void_p, c_void_p]
     lib.img2d_measure_fp32_peak.restype = c_int
     lib.img2d_measure_fp32_peak.argtypes = [POINTER(c_double)]
     lib.img2d_ricker_sources.restype = c_int

@@ -408,6 +408,7 @@ struct img2d_plan {
     long long wave_elems = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     bool ev_recorded = false;
+    bool launched = false;  // a migration kernel has been queued (its status word is initialised)
     ~img2d_plan()
     {
         if (ev0) cudaEventDestroy(ev0);
@@ -657,12 +658,19 @@ static int build_plan(img2d_plan *p, int ns, int nextrap, int nz, int nx, int nf
     // It is the default where the cluster2 kernel's clusters would leave SMs idle (clusters of 4 fit
     // 33 times on 148 SMs), and on request (IMG2D_FLAG_WIDE / _WIDE_SCALAR).
     auto try_wide = [&]() {
-        // with the step-ahead stage where its 12 KB fit (operators up to 49 taps)
-        const bool stage = wide_stage_smem_bytes(M) + static_reserve <= (size_t)smem_optin;
-        const KernelFn wf = (flags & IMG2D_FLAG_WIDE_SCALAR)
-                                ? (stage ? migrate_wide_kernel<0, true> : migrate_wide_kernel<0, false>)
-                                : (stage ? migrate_wide_kernel<1, true> : migrate_wide_kernel<1, false>);
-        const size_t smemw = stage ? wide_stage_smem_bytes(M) : wide_smem_bytes(M);
+        // with the step-ahead stage where its 12 KB fit (operators up to 49 taps); the bulk-copy
+        // ring adds 256 bytes of barriers
+        const bool bulk = (flags & IMG2D_FLAG_WIDE_BULK) != 0;
+        const size_t bars = bulk ? wide_bulk_smem_bytes(M, true) - wide_stage_smem_bytes(M) : 0;
+        const bool stage = wide_stage_smem_bytes(M) + bars + static_reserve <= (size_t)smem_optin;
+        KernelFn wf;
+        if (bulk)
+            wf = stage ? migrate_wide_kernel<1, true, true> : migrate_wide_kernel<1, false, true>;
+        else if (flags & IMG2D_FLAG_WIDE_SCALAR)
+            wf = stage ? migrate_wide_kernel<0, true> : migrate_wide_kernel<0, false>;
+        else
+            wf = stage ? migrate_wide_kernel<1, true> : migrate_wide_kernel<1, false>;
+        const size_t smemw = (stage ? wide_stage_smem_bytes(M) : wide_smem_bytes(M)) + bars;
         if (smemw + static_reserve > (size_t)smem_optin) return false;
         const int widest = make_groups(WideShape::G);
         const int K = (widest + WideShape::PC - 1) / WideShape::PC;
@@ -675,11 +683,15 @@ static int build_plan(img2d_plan *p, int ns, int nextrap, int nz, int nx, int nf
         p->smem = smemw;
         p->max_w = widest;
         p->block = WideShape::NW * 32;
-        p->variant = ((flags & IMG2D_FLAG_WIDE_SCALAR) ? 0 : 1) + (stage ? 2 : 0);
+        p->variant = ((flags & IMG2D_FLAG_WIDE_SCALAR) ? 0 : 1) + (stage ? 2 : 0) + (bulk ? 4 : 0);
         p->kname = "migrate_wide";
         return true;
     };
-    const bool wide_requested = (flags & (IMG2D_FLAG_WIDE | IMG2D_FLAG_WIDE_SCALAR)) != 0;
+    const int wide_flags = IMG2D_FLAG_WIDE | IMG2D_FLAG_WIDE_SCALAR | IMG2D_FLAG_WIDE_BULK;
+    if ((flags & IMG2D_FLAG_WIDE_BULK) && (flags & IMG2D_FLAG_WIDE_SCALAR))
+        return fail(IMG2D_EINVAL, "IMG2D_FLAG_WIDE_BULK runs packed FMAs; it does not combine with "
+                                  "IMG2D_FLAG_WIDE_SCALAR");
+    const bool wide_requested = (flags & wide_flags) != 0;
     const bool wide_ok = mode == OP_CONJ && !tab16 && p->L >= 7 &&
                          !(flags & (IMG2D_FLAG_GENERIC | IMG2D_FLAG_NO_CLUSTER | IMG2D_FLAG_CLUSTER_V1 |
                                     IMG2D_FLAG_CLUSTER2)) &&
@@ -697,7 +709,7 @@ static int build_plan(img2d_plan *p, int ns, int nextrap, int nz, int nx, int nf
         want_wide = p->n_slots < 12 || busy < nsm * 96 / 100;
     }
     if (want_wide) try_wide();
-    if (!p->cluster && cluster_ok && !(flags & (IMG2D_FLAG_CLUSTER_V1 | IMG2D_FLAG_WIDE | IMG2D_FLAG_WIDE_SCALAR)) &&
+    if (!p->cluster && cluster_ok && !(flags & (IMG2D_FLAG_CLUSTER_V1 | wide_flags)) &&
         p->L >= 7) {
         // the default ring variant needs 33 KB more shared memory than the staged one: long
         // operators or very wide windows fall back to the staged variant
@@ -774,7 +786,7 @@ static int build_plan(img2d_plan *p, int ns, int nextrap, int nz, int nx, int nf
     if ((rc = p->segs.ensure(segs.size() * sizeof(int4)))) return rc;
     if ((rc = p->owner.ensure(owner.size() * sizeof(int16_t)))) return rc;
     if ((rc = p->shot_off.ensure(p->off.size() * sizeof(long long)))) return rc;
-    if ((rc = p->counter.ensure(sizeof(int)))) return rc;
+    if ((rc = p->counter.ensure(2 * sizeof(int)))) return rc;  // work-queue counter, status word
     if (p->carver) {
         // ordered on the caller's stream after any earlier call that used the same scratch
         cudaStream_t us = p->upload_stream;
@@ -845,12 +857,26 @@ static MigrateArgs base_args(img2d_plan *p, cpx *wave, cpx *shot)
     return a;
 }
 
+// Status word of the last launch (after the work-queue counter), read on `st` after it.
+static int read_status(img2d_plan *p, cudaStream_t st)
+{
+    int status = 0;
+    IMG2D_CUDA(cudaMemcpyAsync(&status, p->counter.as<int>() + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
+    IMG2D_CUDA(cudaStreamSynchronize(st));
+    if (status)
+        return fail(IMG2D_ECUDA, "a bounded wait in the migration kernel gave up (status " + std::to_string(status) +
+                                     "): the results of that launch are not valid");
+    return IMG2D_OK;
+}
+
 // Launch the persistent kernel and (optionally) reduce the stacked image.
 static int launch(img2d_plan *p, MigrateArgs a, float *d_image, float *d_image_shots,
                   long long img_sstride, cudaStream_t st)
 {
     const size_t plane = (size_t)p->nextrap * p->nx;
-    IMG2D_CUDA(cudaMemsetAsync(p->counter.p, 0, sizeof(int), st));
+    IMG2D_CUDA(cudaMemsetAsync(p->counter.p, 0, 2 * sizeof(int), st));
+    a.status = p->counter.as<int>() + 1;
+    p->launched = true;
     if (d_image) {
         IMG2D_CUDA(cudaMemsetAsync(p->partial.p, 0, (size_t)p->grid * plane * sizeof(float), st));
         IMG2D_CUDA(cudaMemsetAsync(p->comp.p, 0, (size_t)p->grid * plane * sizeof(float), st));
@@ -1399,6 +1425,13 @@ int img2d_plan_kernel_ms(img2d_plan *p, float *ms)
     return IMG2D_OK;
 }
 
+int img2d_plan_status(img2d_plan *p, void *stream)
+{
+    if (!p) return fail(IMG2D_EINVAL, "plan is NULL");
+    if (!p->launched) return fail(IMG2D_EINVAL, "no kernel launched on this plan yet");
+    return img2d::read_status(p, (cudaStream_t)stream);
+}
+
 int img2d_measure_fp32_peak(double *tflops)
 {
     if (!tflops) return fail(IMG2D_EINVAL, "tflops is NULL");
@@ -1722,6 +1755,7 @@ int img2d_migrate_compact(int ns, int nextrap, int nz, int nx, int nf, int nt, i
     MigrateArgs a = base_args(p, dW, dS);
     if ((rc = launch(p, a, dI, dIS, (long long)plane, 0))) return rc;
     IMG2D_CUDA(cudaDeviceSynchronize());
+    if ((rc = read_status(p, 0))) return rc;
     if (image) IMG2D_CUDA(cudaMemcpy(image, dI, (size_t)nextrap * nx * sizeof(float), cudaMemcpyDeviceToHost));
     if (image_shots)
         IMG2D_CUDA(cudaMemcpy2D(image_shots, plane * sizeof(float), dIS, plane * sizeof(float),

@@ -80,6 +80,7 @@ struct MigrateArgs {
     float *image_shots;      // per-shot images (or null), row l of shot s at s*img_sstride + l*nx
     long long img_sstride;
     int *counter;            // work-queue counter, zeroed before launch
+    int *status;             // zeroed before launch; set non-zero by a kernel whose bounded wait gave up
 };
 
 __device__ __forceinline__ int pad_slot(int xl, int X) { return xl + xl / X; }

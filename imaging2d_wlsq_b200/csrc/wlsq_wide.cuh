@@ -29,7 +29,8 @@
 // 16-byte cp.async three tap-loop iterations before they are read.  The next depth step's operator
 // indices and this step's Kahan partial-image values of those two positions reach the thread
 // through a per-thread shared-memory stage filled by cp.async a step ahead (STAGE, where the
-// shared memory allows), or are loaded into registers at the start of the step.
+// shared memory allows), or are loaded into registers at the start of the step.  The BULK variant
+// fills the same ring with 1-D bulk copies completing on per-warp transaction-count barriers.
 //
 // Per depth step: tap loop into registers; aperture mask; edge outputs pushed into the neighbour's
 // halo staging (distributed shared memory, double-buffered by step parity); cluster barrier arrive
@@ -71,6 +72,61 @@ __host__ __device__ inline size_t wide_stage_smem_bytes(int M)
     return wide_smem_bytes(M) + (size_t)WideShape::NW * 32 * kWideStageWords * 4;
 }
 
+// BULK: two transaction-count barriers per warp after the stage words (or the rings), one per
+// alternate ring chunk.
+__host__ __device__ inline size_t wide_bulk_bar_offset(int M, bool stage)
+{
+    return stage ? wide_stage_smem_bytes(M) : wide_smem_bytes(M);
+}
+__host__ __device__ inline size_t wide_bulk_smem_bytes(int M, bool stage)
+{
+    return wide_bulk_bar_offset(M, stage) + (size_t)WideShape::NW * 2 * sizeof(unsigned long long);
+}
+
+// SM clock cycles (about a second) after which a ring-chunk wait gives up: the thread then records
+// the failure in the launch's status word and neither waits for nor issues ring chunks again, so a
+// phase that can never complete ends the launch instead of hanging it.
+constexpr long long kBulkWaitCycles = 1ll << 31;
+
+__device__ __forceinline__ unsigned smem_addr(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(unsigned long long *bar, unsigned count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+
+// the initialisations above become visible to the asynchronous (bulk-copy) proxy
+__device__ __forceinline__ void mbar_init_fence() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+
+// arrive on the barrier's current phase, first raising its expected transaction bytes
+__device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long *bar, unsigned bytes)
+{
+    asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t}" ::"r"(
+                     smem_addr(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, unsigned parity)
+{
+    unsigned done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return done != 0;
+}
+
+// 1-D bulk copy global -> this CTA's shared memory, completing bytes on the barrier (no multicast)
+__device__ __forceinline__ void bulk_copy_g2s(void *dst, const void *src, unsigned bytes, unsigned long long *bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_addr(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_addr(bar))
+                 : "memory");
+}
+
 // float4 column of half h (0 = S, 1 = conj R) of lane q in row pos
 __device__ __forceinline__ int wide_col(int pos, int q, int h) { return 2 * q + (h ^ ((pos >> 3) & 1)); }
 
@@ -103,7 +159,14 @@ __device__ __forceinline__ void wide_mac(float (&c)[8], float fr, float fi, cons
 // STAGE: the next step's operator indices and this step's Kahan values reach the thread through its
 // shared-memory stage words, copied by cp.async one step ahead (no register holds a pending load
 // across the tap loop); otherwise they are loaded into registers at the start of the step.
-template <int ARITH, bool STAGE>
+//
+// BULK: the operator-pair ring is filled by 1-D bulk copies (cp.async.bulk, the copy engine of
+// the SM) instead of per-lane 16-byte cp.async.  Ring iterations are copied in chunks of two (v
+// even: the slots of v and v + 1 are adjacent), one bulk copy of up to 32 bytes per output, each
+// chunk completing on one of two transaction-count barriers of the warp (alternating), where the
+// cp.async ring would wait for a commit group.  A chunk is issued where the cp.async ring copies
+// its later iteration and waited for where the ring waits for its first one.
+template <int ARITH, bool STAGE, bool BULK = false>
 __global__ void __launch_bounds__(WideShape::NW * 32, 1) migrate_wide_kernel(MigrateArgs a)
 {
     using S = WideShape;
@@ -127,6 +190,21 @@ __global__ void __launch_bounds__(WideShape::NW * 32, 1) migrate_wide_kernel(Mig
     unsigned *const sst = reinterpret_cast<unsigned *>(smem + (size_t)(NEXT + 4 * MP) * G + (size_t)S::NG * S::RING) +
                           (size_t)threadIdx.x * kWideStageWords;
     const int npairs = (L + 1) >> 1;
+    static_assert(X == 8 && kRingSlots == 4, "the ring schedule assumes 8 outputs per block and 4 slots");
+    // BULK: this warp's two chunk barriers, the chunks it has issued and waited for (warp-uniform)
+    unsigned long long *const wbar =
+        reinterpret_cast<unsigned long long *>(reinterpret_cast<char *>(smem) + wide_bulk_bar_offset(M, STAGE)) +
+        warp * 2;
+    unsigned n_issued = 0, n_waited = 0;
+    bool bulk_failed = false;
+    if (BULK) {
+        if (lane == 0) {
+            mbar_init(wbar, 32);  // one arrival per lane and chunk
+            mbar_init(wbar + 1, 32);
+            mbar_init_fence();
+        }
+        __syncwarp();
+    }
     const unsigned rank0_item = map_rank(&s_item, 0);
     const int row_bytes = a.tab_stride * 8;
     // register budget (512 threads at <= 128 registers): the partial-image, table and owner
@@ -234,8 +312,56 @@ __global__ void __launch_bounds__(WideShape::NW * 32, 1) migrate_wide_kernel(Mig
             cp_async16_zfill(ringb + q * kRingSlots + sl, tabb + roff0 + (ok0 ? pr0 : 0) * 16, ok0 ? 16u : 0u);
             cp_async16_zfill(ringb + (q + Q) * kRingSlots + sl, tabb + roff1 + (ok1 ? pr1 : 0) * 16, ok1 ? 16u : 0u);
         };
+        // BULK: the pairs of ring iterations v and v + 1 (v even; v + 1 only while <= vlast) of outputs
+        // q and q + 4, one bulk copy per output into the two adjacent slots.  Pairs outside the row
+        // are not copied (their slots are never read).  Every lane arrives on the chunk's barrier
+        // with its own byte count before issuing its copies, so the phase completes only after all
+        // 32 lanes' copies have landed.
+        auto ring_chunk = [&](int v, int vlast) {
+            const char *tabb = reinterpret_cast<const char *>(a.tabF);
+            unsigned long long *bar = wbar + (n_issued & 1);
+            ++n_issued;
+            if (bulk_failed) return;  // never arrive on a phase that may still be open
+            unsigned nb[2];
+            const char *src[2];
+            float4 *dst[2];
+#pragma unroll
+            for (int o = 0; o < 2; ++o) {
+                const int p0 = v + ((X - q - o * Q) >> 1);
+                const bool ok0 = (unsigned)p0 < (unsigned)npairs;
+                const bool ok1 = v + 1 <= vlast && (unsigned)(p0 + 1) < (unsigned)npairs;
+                const int first = ok0 ? 0 : 1;
+                nb[o] = (ok0 ? 16u : 0u) + (ok1 ? 16u : 0u);
+                src[o] = tabb + (o ? roff1 : roff0) + (long long)(p0 + first) * 16;
+                dst[o] = ringb + (q + o * Q) * kRingSlots + (v & (kRingSlots - 1)) + first;
+            }
+            mbar_arrive_expect_tx(bar, nb[0] + nb[1]);
+            if (nb[0]) bulk_copy_g2s(dst[0], src[0], nb[0], bar);
+            if (nb[1]) bulk_copy_g2s(dst[1], src[1], nb[1], bar);
+        };
+        // BULK: wait for the oldest chunk not yet waited for (chunks are waited for in issue order,
+        // and a barrier's next chunk is issued only after its previous one was waited for)
+        auto chunk_wait = [&]() {
+            unsigned long long *bar = wbar + (n_waited & 1);
+            const unsigned parity = (n_waited >> 1) & 1;
+            ++n_waited;
+            if (bulk_failed || mbar_try_wait(bar, parity)) return;
+            const long long t0 = clock64();
+            while (!mbar_try_wait(bar, parity)) {
+                if (clock64() - t0 > kBulkWaitCycles) {
+                    bulk_failed = true;
+                    if (a.status) atomicOr(a.status, 1);
+                    break;
+                }
+            }
+        };
         if (warp_active) {
-            for (int u = -(X / 2); u < 0; ++u) ring_copy(u);
+            if (BULK) {
+                ring_chunk(-4, -1);
+                ring_chunk(-2, -1);
+            } else {
+                for (int u = -(X / 2); u < 0; ++u) ring_copy(u);
+            }
             if (STAGE) {
                 if (a.nextrap > 1) stage_idx(1);
                 stage_kahan(0);
@@ -243,11 +369,16 @@ __global__ void __launch_bounds__(WideShape::NW * 32, 1) migrate_wide_kernel(Mig
         }
         cp_async_commit();
         const int srow0 = b * X + MP - M;  // row of input t = 0
+        const int nmid = (L - X + 1) / 2;  // middle tap-loop iterations (two inputs each)
 
         for (int l = 0; l < a.nextrap; ++l) {
             const int par = l & 1;
             // this step's prologue pairs (copied at the end of the previous step) for the group
             cp_async_wait_all();
+            if (BULK && warp_active) {
+                chunk_wait();
+                chunk_wait();
+            }
             __syncwarp();  // control flow is warp-uniform here
             const long long pe = prow0 + (long long)l * a.nx;
             float cur_s0 = 0.f, cur_c0 = 0.f, cur_s1 = 0.f, cur_c1 = 0.f;
@@ -306,19 +437,29 @@ __global__ void __launch_bounds__(WideShape::NW * 32, 1) migrate_wide_kernel(Mig
                 }
                 // after t = 2u the slot of iteration u - 4 has been read; copy iteration u
                 if ((t & 1) == 0 && (t >> 1) < 3) {
-                    ring_copy(t >> 1);
-                    cp_async_commit();
+                    if (BULK) {
+                        if (t == 2) ring_chunk(0, nmid + 3);
+                    } else {
+                        ring_copy(t >> 1);
+                        cp_async_commit();
+                    }
                 }
             }
             // middle: t = X-1 .. L-1 in steps of two (odd t, then even t+1)
-            const int nmid = (L - X + 1) / 2;
             int row = srow0 + X - 1;
             for (int u = 0; u < nmid; ++u, row += 2) {
                 const float4 *rs = ringb + (u & (kRingSlots - 1));
                 // iteration u - 1 has read the slot of iteration u + 3; wait for iteration u
-                ring_copy(u + 3);
-                cp_async_commit();
-                cp_async_wait<3>();
+                if (BULK) {
+                    if (!(u & 1)) {
+                        ring_chunk(u + 2, nmid + 3);
+                        chunk_wait();
+                    }
+                } else {
+                    ring_copy(u + 3);
+                    cp_async_commit();
+                    cp_async_wait<3>();
+                }
                 __syncwarp();  // control flow is warp-uniform here
                 {
                     float4 va, vb;
@@ -344,19 +485,27 @@ __global__ void __launch_bounds__(WideShape::NW * 32, 1) migrate_wide_kernel(Mig
                 }
             }
             // epilogue: t = L .. L+X-2, outputs jj > t-L are active (k = t - jj <= L-1)
-            ring_copy(nmid + 3);
-            cp_async_commit();
+            if (BULK) {
+                ring_chunk((nmid + 3) & ~1, nmid + 3);
+            } else {
+                ring_copy(nmid + 3);
+                cp_async_commit();
+            }
 #pragma unroll
             for (int e = 0; e < X - 1; ++e) {
                 float4 va, vb;
                 load_in(srow0 + L + e, va, vb);
                 if ((e & 1) == 0) {
                     // steps e and e + 1 read iteration nmid + e / 2; later iterations may be in flight
-                    switch (e >> 1) {
-                        case 0: cp_async_wait<3>(); break;
-                        case 1: cp_async_wait<2>(); break;
-                        case 2: cp_async_wait<1>(); break;
-                        default: cp_async_wait<0>(); break;
+                    if (BULK) {
+                        if (!((nmid + (e >> 1)) & 1)) chunk_wait();
+                    } else {
+                        switch (e >> 1) {
+                            case 0: cp_async_wait<3>(); break;
+                            case 1: cp_async_wait<2>(); break;
+                            case 2: cp_async_wait<1>(); break;
+                            default: cp_async_wait<0>(); break;
+                        }
                     }
                     __syncwarp();  // control flow is warp-uniform here
                 }
@@ -424,7 +573,12 @@ __global__ void __launch_bounds__(WideShape::NW * 32, 1) migrate_wide_kernel(Mig
                     roff0 = (nidx01 & 0xffffu) * (unsigned)row_bytes;
                     roff1 = (nidx01 >> 16) * (unsigned)row_bytes;
                 }
-                for (int u = -(X / 2); u < 0; ++u) ring_copy(u);
+                if (BULK) {
+                    ring_chunk(-4, -1);
+                    ring_chunk(-2, -1);
+                } else {
+                    for (int u = -(X / 2); u < 0; ++u) ring_copy(u);
+                }
                 // the words just read are refilled for step l + 2 (their reads are complete: the
                 // copies above used them)
                 if (STAGE && l + 2 < a.nextrap) stage_idx(l + 2);

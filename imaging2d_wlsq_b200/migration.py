@@ -16,7 +16,7 @@ from ._lib import check, lib, ptr
 def migrate(ns, nextrap, nz, nx, nf, nt, M, nk, dk, omega, velocity, tab_forw, wave_fs, shot_fs,
             tab_back=None, shot_x0=None, shot_nx=None, image=True, image_shots=False, two_tables=False,
             generic=False, no_cluster=False, cluster_v1=False, variant=0, wide=False, wide_scalar=False,
-            cluster2=False):
+            cluster2=False, wide_bulk=False):
     """Host-buffer migration.  wave_fs/shot_fs (packed complex64) are overwritten with the final
     wavefields.  Returns (image (nz, nx) float32 or None, image_shots (ns, nz, nx) or None); rows
     [nextrap, nz) are zero.  variant: cluster-kernel variant (1-based, 0 = default)."""
@@ -34,7 +34,7 @@ def migrate(ns, nextrap, nz, nx, nf, nt, M, nk, dk, omega, velocity, tab_forw, w
     imgs = np.zeros((ns, nz, nx), dtype=np.float32) if image_shots else None
     flags = (_lib.FLAG_TWO_TABLES if two_tables else 0) | (_lib.FLAG_GENERIC if generic else 0) | \
         (_lib.FLAG_NO_CLUSTER if no_cluster else 0) | (_lib.FLAG_CLUSTER_V1 if cluster_v1 else 0) | \
-        (int(variant) << _lib.FLAG_VARIANT_SHIFT) | _wide_flags(wide, wide_scalar) | \
+        (int(variant) << _lib.FLAG_VARIANT_SHIFT) | _wide_flags(wide, wide_scalar, wide_bulk) | \
         (_lib.FLAG_CLUSTER2 if cluster2 else 0)
     check(lib().img2d_migrate_compact(ns, nextrap, nz, nx, nf, nt, M, nk, float(dk), ptr(omega), ptr(velocity),
                                       ptr(tab_forw), ptr(tab_back), ptr(x0), ptr(wn), ptr(wave_fs), ptr(shot_fs),
@@ -43,7 +43,7 @@ def migrate(ns, nextrap, nz, nx, nf, nt, M, nk, dk, omega, velocity, tab_forw, w
 
 
 def migrate_workload(w, two_tables=False, table_back=None, image_shots=False, generic=False, no_cluster=False,
-                     cluster_v1=False, variant=0, wide=False, wide_scalar=False, cluster2=False):
+                     cluster_v1=False, variant=0, wide=False, wide_scalar=False, cluster2=False, wide_bulk=False):
     """Run a synthetic.Workload through the host entry point on copies of its spectra."""
     wave = w.wave.copy()
     shot = w.shot.copy()
@@ -51,27 +51,27 @@ def migrate_workload(w, two_tables=False, table_back=None, image_shots=False, ge
                         wave, shot, tab_back=table_back, shot_x0=w.shot_x0, shot_nx=w.shot_nx,
                         image_shots=image_shots, two_tables=two_tables, generic=generic, no_cluster=no_cluster,
                         cluster_v1=cluster_v1, variant=variant, wide=wide, wide_scalar=wide_scalar,
-                        cluster2=cluster2)
+                        cluster2=cluster2, wide_bulk=wide_bulk)
     return img, imgs, wave, shot
 
 
 def plan_flags(two_tables=False, generic=False, no_cluster=False, cluster_v1=False, variant=0, table="fp32",
-               demig_ring=True, wide=False, wide_scalar=False, cluster2=False):
+               demig_ring=True, wide=False, wide_scalar=False, cluster2=False, wide_bulk=False):
     """The C ABI `flags` word of a kernel configuration given as Plan keyword arguments."""
     return (_lib.FLAG_TWO_TABLES if two_tables else 0) | (_lib.FLAG_GENERIC if generic else 0) | \
         (_lib.FLAG_NO_CLUSTER if no_cluster else 0) | (_lib.FLAG_CLUSTER_V1 if cluster_v1 else 0) | \
         (int(variant) << _lib.FLAG_VARIANT_SHIFT) | \
         {"fp32": 0, "fp16": _lib.FLAG_TABLE_FP16, "bf16": _lib.FLAG_TABLE_BF16}[table] | \
-        (0 if demig_ring else _lib.FLAG_DEMIG_NO_RING) | _wide_flags(wide, wide_scalar) | \
+        (0 if demig_ring else _lib.FLAG_DEMIG_NO_RING) | _wide_flags(wide, wide_scalar, wide_bulk) | \
         (_lib.FLAG_CLUSTER2 if cluster2 else 0)
 
 
-def _wide_flags(wide, wide_scalar):
+def _wide_flags(wide, wide_scalar, wide_bulk=False):
     """Flags of the wide cluster kernel (8 slots x 1024 positions per CTA): packed FMAs by default,
-    scalar FMAs with wide_scalar."""
-    if not (wide or wide_scalar):
+    scalar FMAs with wide_scalar, the operator-pair ring filled by 1-D bulk copies with wide_bulk."""
+    if not (wide or wide_scalar or wide_bulk):
         return 0
-    return _lib.FLAG_WIDE | (_lib.FLAG_WIDE_SCALAR if wide_scalar else 0)
+    return _lib.FLAG_WIDE | (_lib.FLAG_WIDE_SCALAR if wide_scalar else 0) | (_lib.FLAG_WIDE_BULK if wide_bulk else 0)
 
 
 def fp32_peak_tflops():
@@ -93,7 +93,7 @@ class Plan:
 
     def __init__(self, ns, nextrap, nz, nx, nf, nt, M, nk, shot_x0=None, shot_nx=None, two_tables=False,
                  generic=False, no_cluster=False, cluster_v1=False, variant=0, table="fp32", demig_ring=True,
-                 wide=False, wide_scalar=False, cluster2=False):
+                 wide=False, wide_scalar=False, cluster2=False, wide_bulk=False):
         """table: operator-table storage, "fp32" (default), "fp16" or "bf16" (reduced-precision
         storage, FP32 arithmetic; cluster kernel only).  demig_ring: the cluster demigration kernel's
         forward steps read their operator pairs through a shared-memory ring (False: through L1)."""
@@ -102,7 +102,7 @@ class Plan:
         x0 = None if shot_x0 is None else np.ascontiguousarray(shot_x0, dtype=np.int32)
         wn = None if shot_nx is None else np.ascontiguousarray(shot_nx, dtype=np.int32)
         flags = plan_flags(two_tables, generic, no_cluster, cluster_v1, variant, table, demig_ring, wide, wide_scalar,
-                           cluster2)
+                           cluster2, wide_bulk)
         h = ctypes.c_void_p()
         check(lib().img2d_plan_create(ctypes.byref(h), ns, nextrap, nz, nx, nf, nt, M, nk, ptr(x0), ptr(wn), flags))
         self._h = h
@@ -176,6 +176,11 @@ class Plan:
         check(lib().img2d_plan_kernel_ms(self._h, ctypes.byref(v)))
         return v.value
 
+    def check_status(self, stream=None):
+        """Raise LibraryError if a bounded wait inside the last migration kernel gave up (its results
+        are then invalid); waits for that kernel."""
+        check(lib().img2d_plan_status(self._h, self._stream(stream)))
+
     def shot_offset(self, s):
         return lib().img2d_plan_shot_offset(self._h, s)
 
@@ -202,7 +207,8 @@ class Plan:
 # operator indices, Kahan rows and tap pairs reach the tap loop (L1, shared-memory stage or ring).
 N_CLUSTER2_VARIANTS = 12
 CANDIDATES = [("default", {})] + [("cluster2/v%d" % v, {"variant": v}) for v in range(1, N_CLUSTER2_VARIANTS + 1)] + \
-             [("wide/ffma2", {"wide": True}), ("wide/ffma", {"wide_scalar": True}), ("cluster2", {"cluster2": True}),
+             [("wide/ffma2", {"wide": True}), ("wide/ffma", {"wide_scalar": True}), ("wide/bulk", {"wide_bulk": True}),
+              ("cluster2", {"cluster2": True}),
               ("cluster1", {"cluster_v1": True}), ("single-cta", {"no_cluster": True})]
 
 
@@ -241,6 +247,11 @@ def autotune(ns, nextrap, nz, nx, nf, nt, M, nk, dk, omega, velocity, table, wav
         for _ in range(repeats + 1):
             plan.execute(w2, s2, img)
             times.append(plan.kernel_ms())
+        try:
+            plan.check_status()
+        except LibraryError:
+            plan.close()
+            continue
         table_rows.append((min(times[1:]), name, d, kw))
         plan.close()
     if not table_rows:

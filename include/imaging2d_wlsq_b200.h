@@ -44,6 +44,9 @@ typedef struct {
 #define IMG2D_FLAG_WIDE 128        /* wide cluster kernel: 8 slots x 1024 positions per CTA (packed FMAs) */
 #define IMG2D_FLAG_WIDE_SCALAR (1 << 16) /* the wide cluster kernel with scalar instead of packed FMAs */
 #define IMG2D_FLAG_CLUSTER2 (1 << 17)    /* 16-slot cluster kernel (512 positions per CTA) instead */
+/* the wide cluster kernel (packed FMAs) with its operator-pair ring filled by 1-D bulk copies
+ * (cp.async.bulk, completing on per-warp transaction barriers) instead of 16-byte cp.async */
+#define IMG2D_FLAG_WIDE_BULK (1 << 18)
 /* Default kernel choice: the wide cluster kernel where the 16-slot kernel's clusters would leave
  * SMs idle (or fewer than 12 lane slots), else the 16-slot cluster kernel; the single-CTA kernels
  * for fewer than 6 lane slots, operators shorter than 7 taps or windows beyond 16 CTAs. */
@@ -146,6 +149,12 @@ void img2d_plan_destroy(img2d_plan *plan);
 /* Device time (ms) of the persistent migration kernel alone in the last img2d_plan_execute on this
  * plan, from CUDA events recorded around that launch on its stream (waits for it to finish). */
 int img2d_plan_kernel_ms(img2d_plan *plan, float *ms);
+
+/* Status of the last migration launch on this plan, read on `stream` after it (waits for it):
+ * IMG2D_ECUDA if a bounded wait inside the kernel gave up (the bulk-copy ring of
+ * IMG2D_FLAG_WIDE_BULK; the results of that launch are then invalid), else IMG2D_OK.
+ * img2d_migrate_compact checks it by itself. */
+int img2d_plan_status(img2d_plan *plan, void *stream);
 
 /* FP32 FMA throughput of the current device in TFLOP/s, measured by a short kernel of independent
  * FMA chains (the denominator of the FP32 roofline; not part of the migration path). */

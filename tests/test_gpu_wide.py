@@ -1,8 +1,9 @@
 """The wide cluster kernel (8 lane slots x 1024 positions per CTA, clusters of half the size of the
 cluster2 kernel's, each item's window split evenly over its CTAs) against the FP64 oracle
 (relative L2 1e-5, the compact-path bar), in both its packed (FFMA2) and scalar FMA forms, with
-and without the step-ahead stage, and bit for bit against the cluster2 kernel's final wavefields
-(the same FMA sequence per element)."""
+and without the step-ahead stage, with its operator-pair ring filled by 16-byte cp.async or by 1-D
+bulk copies, and bit for bit against the cluster2 kernel's final wavefields (the same FMA sequence
+per element)."""
 import numpy as np
 import pytest
 
@@ -12,7 +13,8 @@ from tests.conftest import rel_l2
 
 pytestmark = pytest.mark.gpu
 
-ARITH = [dict(wide=True), dict(wide_scalar=True)]
+ARITH = [dict(wide=True), dict(wide_scalar=True), dict(wide_bulk=True)]
+IDS = ["ffma2", "ffma", "bulk"]
 
 
 def _with_M(w, M):
@@ -35,7 +37,7 @@ CASES = {
 
 
 @pytest.mark.parametrize("case", list(CASES))
-@pytest.mark.parametrize("arith", ARITH, ids=["ffma2", "ffma"])
+@pytest.mark.parametrize("arith", ARITH, ids=IDS)
 def test_wide_matches_fp64_oracle(case, arith):
     w = CASES[case]()
     d = migration.Plan.for_workload(w, **arith).describe()
@@ -47,7 +49,7 @@ def test_wide_matches_fp64_oracle(case, arith):
     assert np.all(img[w.nextrap:] == 0)
 
 
-@pytest.mark.parametrize("arith", ARITH, ids=["ffma2", "ffma"])
+@pytest.mark.parametrize("arith", ARITH, ids=IDS)
 def test_wide_wavefields_bitwise_equal_cluster2(arith):
     w = synthetic.batched_uneven(scale=0.1)
     assert migration.Plan.for_workload(w, cluster2=True).describe()["kernel"] == "migrate_cluster2"
@@ -97,3 +99,35 @@ def test_default_kernel_choice():
     assert migration.Plan.for_workload(w).describe()["kernel"] == "migrate_wide"
     w = synthetic.plain_medium(nz=6, nf=2)  # 32 full-aperture shots over 1024 positions: clusters of 2
     assert migration.Plan.for_workload(w).describe()["kernel"] == "migrate_cluster2"
+
+
+def test_wide_bulk_plan_and_status():
+    """The bulk-copy ring is a variant of the wide kernel (variant bit 4, with and without the
+    stage), its launches report a clean status word, it gives the same wavefields as the cp.async
+    ring, and it rejects the scalar-FMA flag."""
+    import torch
+    from imaging2d_wlsq_b200._lib import LibraryError
+    w = synthetic.batched_uneven(scale=0.08)
+    d = migration.Plan.for_workload(w, wide_bulk=True).describe()
+    assert d["kernel"] == "migrate_wide" and d["variant"] == 7, d  # packed FMAs + stage + bulk
+    w81 = CASES["uneven_L81"]()
+    assert migration.Plan.for_workload(w81, wide_bulk=True).describe()["variant"] == 5  # no stage
+    with pytest.raises(LibraryError):
+        migration.Plan.for_workload(w, wide_bulk=True, wide_scalar=True)
+    dev = torch.device("cuda")
+    out = []
+    for kw in (dict(wide=True), dict(wide_bulk=True)):
+        plan = migration.Plan.for_workload(w, **kw)
+        plan.set_model(torch.from_numpy(w.omega).to(dev),
+                       torch.from_numpy(np.ascontiguousarray(w.velocity)).to(dev), w.dk,
+                       torch.from_numpy(w.table).to(dev))
+        wave = torch.from_numpy(w.wave.copy()).to(dev)
+        shot = torch.from_numpy(w.shot.copy()).to(dev)
+        img = torch.zeros((w.nz, w.nx), dtype=torch.float32, device=dev)
+        plan.execute(wave, shot, img)
+        plan.check_status()
+        out.append((wave.cpu().numpy(), shot.cpu().numpy(), img.cpu().numpy()))
+        plan.close()
+    np.testing.assert_array_equal(out[1][0], out[0][0])
+    np.testing.assert_array_equal(out[1][1], out[0][1])
+    assert rel_l2(out[1][2], out[0][2]) <= 1e-6
