@@ -76,8 +76,8 @@ def parse_args():
     p.add_argument("--no-frontend", action="store_true", help="skip the front-end (wavelet, record spectra) leg")
     p.add_argument("--no-accuracy", action="store_true",
                    help="skip the rel-L2 check of the image against the FP64 checker on a sub-volume")
-    p.add_argument("--kernel", default="auto", choices=["auto", "cluster2", "wide", "wide-scalar", "wide-bulk", "cluster1",
-                                                           "single"],
+    p.add_argument("--kernel", default="auto", choices=["auto", "cluster2", "wide", "wide-scalar", "wide-bulk", "wide-lines",
+                                                           "cluster1", "single"],
                    help="kernel family (comparison runs and profiling); auto = the autotuner's choice")
     return p.parse_args()
 
@@ -540,8 +540,9 @@ def main():
                        "ms": {n: round(t, 3) for t, n, _ in rows}}
     else:
         best = dict(no_cluster=args.kernel == "single", cluster_v1=args.kernel == "cluster1", variant=args.variant,
-                    wide=args.kernel == "wide", wide_scalar=args.kernel == "wide-scalar",
-                    wide_bulk=args.kernel == "wide-bulk", cluster2=args.kernel == "cluster2")
+                    wide=args.kernel in ("wide", "wide-lines"), wide_scalar=args.kernel == "wide-scalar",
+                    wide_bulk=args.kernel == "wide-bulk", cluster2=args.kernel == "cluster2",
+                    line_packing=args.kernel == "wide-lines")
     plan = migration.Plan.for_workload(w, **best)
     plan.set_model(om, vel, w.dk, tab)
     wave = torch.empty_like(wave0)

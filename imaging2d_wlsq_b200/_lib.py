@@ -33,6 +33,7 @@ FLAG_WIDE = 128
 FLAG_WIDE_SCALAR = 1 << 16
 FLAG_CLUSTER2 = 1 << 17
 FLAG_WIDE_BULK = 1 << 18
+FLAG_LINE_PACKING = 1 << 19
 NOALLOC_SCRATCH_BYTES = 64 << 20
 
 ERROR_NAMES = {1: "EINVAL", 2: "ENOMEM", 3: "ECUDA", 4: "ENODEV"}

@@ -409,6 +409,8 @@ struct img2d_plan {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     bool ev_recorded = false;
     bool launched = false;  // a migration kernel has been queued (its status word is initialised)
+    const char *packing = "lines";  // how shots were packed into the wide kernel's items
+    double pack_cost = 0.0;         // wide kernel: modelled cost of all items of one frequency, in CTA units
     ~img2d_plan()
     {
         if (ev0) cudaEventDestroy(ev0);
@@ -498,6 +500,34 @@ static size_t smem_bytes(int G, int W, int M, int X)
     return 2 * nslot * G * sizeof(float4);
 }
 
+// One group from its lines (each a list of shots, in increasing x, separated by >= M zero samples).
+static void emit_group(const img2d_plan *p, const std::vector<std::vector<int>> &lines, std::vector<GroupDesc> &groups,
+                       std::vector<int4> &segs, std::vector<int16_t> &owner)
+{
+    int u0 = p->nx, u1 = 0;
+    for (const auto &line : lines)
+        for (int s : line) {
+            u0 = std::min(u0, p->x0[s]);
+            u1 = std::max(u1, p->x0[s] + p->w[s]);
+        }
+    GroupDesc gd{};
+    gd.seg_begin = (int)segs.size();
+    gd.u0 = u0;
+    gd.W = u1 - u0;
+    gd.nslots = (int)lines.size();
+    gd.owner_stride = (gd.W + 7) / 8 * 8;
+    gd.owner_off = (long long)owner.size();
+    owner.resize(owner.size() + (size_t)gd.nslots * gd.owner_stride, (int16_t)-1);
+    for (int k = 0; k < gd.nslots; ++k)
+        for (int s : lines[k]) {
+            segs.push_back(make_int4(s, k, p->x0[s], p->w[s]));
+            int16_t *row = owner.data() + gd.owner_off + (size_t)k * gd.owner_stride;
+            for (int x = p->x0[s]; x < p->x0[s] + p->w[s]; ++x) row[x - u0] = (int16_t)s;
+        }
+    gd.nseg = (int)segs.size() - gd.seg_begin;
+    groups.push_back(gd);
+}
+
 // Slots of similar extent form groups of G that share a work item; returns the widest group.
 static int pack_groups(const img2d_plan *p, int G, std::vector<GroupDesc> &groups, std::vector<int4> &segs,
                        std::vector<int16_t> &owner)
@@ -509,32 +539,133 @@ static int pack_groups(const img2d_plan *p, int G, std::vector<GroupDesc> &group
     const std::vector<int> &sorder = p->slot_order;
     for (size_t g0 = 0; g0 < sorder.size(); g0 += G) {
         const int n = (int)std::min<size_t>(G, sorder.size() - g0);
-        int u0 = p->nx, u1 = 0;
-        for (int k = 0; k < n; ++k) {
-            const int i = sorder[g0 + k];
-            u0 = std::min(u0, p->x0[p->slots[i].front()]);
-            u1 = std::max(u1, p->slot_end[i]);
-        }
-        GroupDesc gd{};
-        gd.seg_begin = (int)segs.size();
-        gd.u0 = u0;
-        gd.W = u1 - u0;
-        gd.nslots = n;
-        gd.owner_stride = (gd.W + 7) / 8 * 8;
-        gd.owner_off = (long long)owner.size();
-        owner.resize(owner.size() + (size_t)n * gd.owner_stride, (int16_t)-1);
-        for (int k = 0; k < n; ++k) {
-            for (int s : p->slots[sorder[g0 + k]]) {
-                segs.push_back(make_int4(s, k, p->x0[s], p->w[s]));
-                int16_t *row = owner.data() + gd.owner_off + (size_t)k * gd.owner_stride;
-                for (int x = p->x0[s]; x < p->x0[s] + p->w[s]; ++x) row[x - u0] = (int16_t)s;
-            }
-        }
-        gd.nseg = (int)segs.size() - gd.seg_begin;
-        groups.push_back(gd);
-        widest = std::max(widest, gd.W);
+        std::vector<std::vector<int>> lines;
+        for (int k = 0; k < n; ++k) lines.push_back(p->slots[sorder[g0 + k]]);
+        emit_group(p, lines, groups, segs, owner);
+        widest = std::max(widest, groups.back().W);
     }
     return widest;
+}
+
+// Wide kernel (8 slots x 1024 positions per CTA, clusters of K CTAs, each item's window split
+// evenly over the cluster in 256-position units): cost of one item of width W in CTA units (one
+// CTA, one depth step, all 1024 positions), divided by the throughput of a CTA with NC/64 busy
+// warps relative to 16.  The relative throughputs are measured on a B200 (16 busy warps against 8:
+// 7.15e10 against 6.19e10 points/s on equal work); the 4- and 12-warp figures are interpolated.
+static double wide_item_cost(int W, int K)
+{
+    const int NC = std::min(WideShape::PC, (W + K * 256 - 1) / (K * 256) * 256);
+    const double eff = NC >= 1024 ? 1.0 : (NC >= 768 ? 0.95 : (NC >= 512 ? 0.875 : 0.6));
+    return (double)K * NC / WideShape::PC / eff;
+}
+
+// Up to G lines of shots inside [u0, u1) from `pool` (shots sorted by aperture end): each line is
+// the heaviest chain of shots (total aperture width) separated by >= M, taken in turn (weighted
+// interval scheduling, repeated).  Returns the aperture width covered; the lines when asked.
+static long long window_lines(const img2d_plan *p, const std::vector<int> &pool, int u0, int u1, int G,
+                              std::vector<std::vector<int>> *lines_out)
+{
+    std::vector<int> cand;
+    for (int s : pool)
+        if (p->x0[s] >= u0 && p->x0[s] + p->w[s] <= u1) cand.push_back(s);
+    long long covered = 0;
+    std::vector<long long> best, ends;
+    std::vector<int> prev;
+    std::vector<char> take;
+    for (int line = 0; line < G && !cand.empty(); ++line) {
+        const int n = (int)cand.size();
+        ends.resize(n);
+        best.assign(n + 1, 0);
+        prev.resize(n);
+        take.assign(n, 0);
+        for (int i = 0; i < n; ++i) ends[i] = (long long)p->x0[cand[i]] + p->w[cand[i]] + p->M;
+        for (int i = 0; i < n; ++i) {
+            const int s = cand[i];
+            // shots before i that end (with the M gap) at or before this one's start
+            const int j = (int)(std::upper_bound(ends.begin(), ends.begin() + i, (long long)p->x0[s]) - ends.begin());
+            prev[i] = j;
+            const long long with = best[j] + p->w[s];
+            if (with > best[i]) {
+                best[i + 1] = with;
+                take[i] = 1;
+            } else {
+                best[i + 1] = best[i];
+            }
+        }
+        std::vector<int> chosen;
+        std::vector<char> used(n, 0);
+        for (int i = n; i > 0;) {
+            if (take[i - 1]) {
+                chosen.push_back(cand[i - 1]);
+                used[i - 1] = 1;
+                i = prev[i - 1];
+            } else {
+                --i;
+            }
+        }
+        covered += best[n];
+        if (lines_out) {
+            std::reverse(chosen.begin(), chosen.end());
+            lines_out->push_back(chosen);
+        }
+        std::vector<int> rest;
+        for (int i = 0; i < n; ++i)
+            if (!used[i]) rest.push_back(cand[i]);
+        cand.swap(rest);
+    }
+    return covered;
+}
+
+// Window-first packing for the wide kernel: repeatedly take the window (a start on a 32-position
+// grid and a width of K x 256 x m positions, m = 1..4, the widths at which an item's cost steps)
+// whose G best lines of the remaining shots cover the most aperture per unit of cost, until every
+// shot is placed.  Narrow windows become narrow items, which the kernel runs with fewer busy warps
+// instead of computing positions outside every aperture.  Returns the total cost in CTA units.
+static double pack_groups_windows(const img2d_plan *p, int G, int K, std::vector<GroupDesc> &groups,
+                                  std::vector<int4> &segs, std::vector<int16_t> &owner)
+{
+    groups.clear();
+    segs.clear();
+    owner.clear();
+    std::vector<int> pool(p->ns);
+    std::iota(pool.begin(), pool.end(), 0);
+    std::stable_sort(pool.begin(), pool.end(),
+                     [&](int a, int b) { return p->x0[a] + p->w[a] < p->x0[b] + p->w[b]; });
+    const int nx = p->nx;
+    const int step = std::max(32, (nx / 64 + 31) / 32 * 32);
+    double total = 0.0;
+    while (!pool.empty()) {
+        double best_ratio = -1.0;
+        int best_u0 = 0, best_w = 0;
+        for (int m = 1; m <= 4; ++m) {
+            const int W = std::min(nx, K * 256 * m);
+            const double c = wide_item_cost(W, K);
+            for (int u = 0;; u += step) {
+                const int u0 = std::min(u, nx - W);
+                const long long cov = window_lines(p, pool, u0, u0 + W, G, nullptr);
+                if (cov > 0 && cov / c > best_ratio) {
+                    best_ratio = cov / c;
+                    best_u0 = u0;
+                    best_w = W;
+                }
+                if (u0 >= nx - W) break;
+            }
+            if (W >= nx) break;
+        }
+        if (best_ratio <= 0.0) return -1.0;  // a shot wider than every window (not reached: K covers it)
+        std::vector<std::vector<int>> lines;
+        window_lines(p, pool, best_u0, best_u0 + best_w, G, &lines);
+        emit_group(p, lines, groups, segs, owner);
+        total += wide_item_cost(groups.back().W, K);
+        std::vector<char> placed(p->ns, 0);
+        for (const auto &line : lines)
+            for (int s : line) placed[s] = 1;
+        std::vector<int> rest;
+        for (int s : pool)
+            if (!placed[s]) rest.push_back(s);
+        pool.swap(rest);
+    }
+    return total;
 }
 
 static int build_plan(img2d_plan *p, int ns, int nextrap, int nz, int nx, int nf, int nt, int M,
@@ -672,8 +803,29 @@ static int build_plan(img2d_plan *p, int ns, int nextrap, int nz, int nx, int nf
             wf = stage ? migrate_wide_kernel<1, true> : migrate_wide_kernel<1, false>;
         const size_t smemw = (stage ? wide_stage_smem_bytes(M) : wide_smem_bytes(M)) + bars;
         if (smemw + static_reserve > (size_t)smem_optin) return false;
-        const int widest = make_groups(WideShape::G);
-        const int K = (widest + WideShape::PC - 1) / WideShape::PC;
+        int widest = make_groups(WideShape::G);
+        int K = (widest + WideShape::PC - 1) / WideShape::PC;
+        p->packing = "lines";
+        p->pack_cost = 0.0;
+        for (const GroupDesc &g : groups) p->pack_cost += wide_item_cost(g.W, K);
+        if (!(flags & IMG2D_FLAG_LINE_PACKING)) {
+            // window-first packing where it costs less, on clusters just wide enough for the widest shot
+            const int Kw = (*std::max_element(p->w.begin(), p->w.end()) + WideShape::PC - 1) / WideShape::PC;
+            std::vector<GroupDesc> g2;
+            std::vector<int4> s2;
+            std::vector<int16_t> o2;
+            const double cost2 = pack_groups_windows(p, WideShape::G, Kw, g2, s2, o2);
+            if (cost2 > 0.0 && cost2 < p->pack_cost * 0.99) {
+                groups.swap(g2);
+                segs.swap(s2);
+                owner.swap(o2);
+                K = Kw;
+                widest = 0;
+                for (const GroupDesc &g : groups) widest = std::max(widest, g.W);
+                p->packing = "windows";
+                p->pack_cost = cost2;
+            }
+        }
         if (!(K <= 8 || (K <= kMaxCluster && clusters_that_fit((const void *)wf, K, WideShape::NW * 32, smemw) > 0)))
             return false;
         p->cluster = K;
@@ -1407,10 +1559,10 @@ int img2d_plan_describe(const img2d_plan *p, char *buf, int buflen)
     snprintf(buf, buflen,
              "{\"kernel\": \"%s\", \"cluster\": %d, \"G\": %d, \"X\": %d, \"L\": %d, \"grid\": %d, \"block\": %d, "
              "\"smem\": %zu, \"items\": %d, \"slots\": %d, \"max_union_width\": %d, \"mode\": %d, \"variant\": %d, "
-             "\"table\": \"%s\"}",
+             "\"table\": \"%s\", \"packing\": \"%s\", \"cost_units\": %.3f}",
              p->kname, p->cluster, p->G, p->fixed ? kX : 4, p->L, p->grid, p->block, p->smem,
              p->n_items, p->n_slots, p->max_w, p->mode, p->variant,
-             p->tab16 == 2 ? "bf16" : (p->tab16 == 1 ? "fp16" : "fp32"));
+             p->tab16 == 2 ? "bf16" : (p->tab16 == 1 ? "fp16" : "fp32"), p->packing, p->pack_cost);
     return IMG2D_OK;
 }
 

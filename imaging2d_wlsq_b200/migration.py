@@ -16,7 +16,7 @@ from ._lib import check, lib, ptr
 def migrate(ns, nextrap, nz, nx, nf, nt, M, nk, dk, omega, velocity, tab_forw, wave_fs, shot_fs,
             tab_back=None, shot_x0=None, shot_nx=None, image=True, image_shots=False, two_tables=False,
             generic=False, no_cluster=False, cluster_v1=False, variant=0, wide=False, wide_scalar=False,
-            cluster2=False, wide_bulk=False):
+            cluster2=False, wide_bulk=False, line_packing=False):
     """Host-buffer migration.  wave_fs/shot_fs (packed complex64) are overwritten with the final
     wavefields.  Returns (image (nz, nx) float32 or None, image_shots (ns, nz, nx) or None); rows
     [nextrap, nz) are zero.  variant: cluster-kernel variant (1-based, 0 = default)."""
@@ -35,7 +35,7 @@ def migrate(ns, nextrap, nz, nx, nf, nt, M, nk, dk, omega, velocity, tab_forw, w
     flags = (_lib.FLAG_TWO_TABLES if two_tables else 0) | (_lib.FLAG_GENERIC if generic else 0) | \
         (_lib.FLAG_NO_CLUSTER if no_cluster else 0) | (_lib.FLAG_CLUSTER_V1 if cluster_v1 else 0) | \
         (int(variant) << _lib.FLAG_VARIANT_SHIFT) | _wide_flags(wide, wide_scalar, wide_bulk) | \
-        (_lib.FLAG_CLUSTER2 if cluster2 else 0)
+        (_lib.FLAG_CLUSTER2 if cluster2 else 0) | (_lib.FLAG_LINE_PACKING if line_packing else 0)
     check(lib().img2d_migrate_compact(ns, nextrap, nz, nx, nf, nt, M, nk, float(dk), ptr(omega), ptr(velocity),
                                       ptr(tab_forw), ptr(tab_back), ptr(x0), ptr(wn), ptr(wave_fs), ptr(shot_fs),
                                       ptr(img), ptr(imgs), flags))
@@ -43,7 +43,8 @@ def migrate(ns, nextrap, nz, nx, nf, nt, M, nk, dk, omega, velocity, tab_forw, w
 
 
 def migrate_workload(w, two_tables=False, table_back=None, image_shots=False, generic=False, no_cluster=False,
-                     cluster_v1=False, variant=0, wide=False, wide_scalar=False, cluster2=False, wide_bulk=False):
+                     cluster_v1=False, variant=0, wide=False, wide_scalar=False, cluster2=False, wide_bulk=False,
+                     line_packing=False):
     """Run a synthetic.Workload through the host entry point on copies of its spectra."""
     wave = w.wave.copy()
     shot = w.shot.copy()
@@ -51,19 +52,20 @@ def migrate_workload(w, two_tables=False, table_back=None, image_shots=False, ge
                         wave, shot, tab_back=table_back, shot_x0=w.shot_x0, shot_nx=w.shot_nx,
                         image_shots=image_shots, two_tables=two_tables, generic=generic, no_cluster=no_cluster,
                         cluster_v1=cluster_v1, variant=variant, wide=wide, wide_scalar=wide_scalar,
-                        cluster2=cluster2, wide_bulk=wide_bulk)
+                        cluster2=cluster2, wide_bulk=wide_bulk, line_packing=line_packing)
     return img, imgs, wave, shot
 
 
 def plan_flags(two_tables=False, generic=False, no_cluster=False, cluster_v1=False, variant=0, table="fp32",
-               demig_ring=True, wide=False, wide_scalar=False, cluster2=False, wide_bulk=False):
+               demig_ring=True, wide=False, wide_scalar=False, cluster2=False, wide_bulk=False,
+               line_packing=False):
     """The C ABI `flags` word of a kernel configuration given as Plan keyword arguments."""
     return (_lib.FLAG_TWO_TABLES if two_tables else 0) | (_lib.FLAG_GENERIC if generic else 0) | \
         (_lib.FLAG_NO_CLUSTER if no_cluster else 0) | (_lib.FLAG_CLUSTER_V1 if cluster_v1 else 0) | \
         (int(variant) << _lib.FLAG_VARIANT_SHIFT) | \
         {"fp32": 0, "fp16": _lib.FLAG_TABLE_FP16, "bf16": _lib.FLAG_TABLE_BF16}[table] | \
         (0 if demig_ring else _lib.FLAG_DEMIG_NO_RING) | _wide_flags(wide, wide_scalar, wide_bulk) | \
-        (_lib.FLAG_CLUSTER2 if cluster2 else 0)
+        (_lib.FLAG_CLUSTER2 if cluster2 else 0) | (_lib.FLAG_LINE_PACKING if line_packing else 0)
 
 
 def _wide_flags(wide, wide_scalar, wide_bulk=False):
@@ -93,7 +95,7 @@ class Plan:
 
     def __init__(self, ns, nextrap, nz, nx, nf, nt, M, nk, shot_x0=None, shot_nx=None, two_tables=False,
                  generic=False, no_cluster=False, cluster_v1=False, variant=0, table="fp32", demig_ring=True,
-                 wide=False, wide_scalar=False, cluster2=False, wide_bulk=False):
+                 wide=False, wide_scalar=False, cluster2=False, wide_bulk=False, line_packing=False):
         """table: operator-table storage, "fp32" (default), "fp16" or "bf16" (reduced-precision
         storage, FP32 arithmetic; cluster kernel only).  demig_ring: the cluster demigration kernel's
         forward steps read their operator pairs through a shared-memory ring (False: through L1)."""
@@ -102,7 +104,7 @@ class Plan:
         x0 = None if shot_x0 is None else np.ascontiguousarray(shot_x0, dtype=np.int32)
         wn = None if shot_nx is None else np.ascontiguousarray(shot_nx, dtype=np.int32)
         flags = plan_flags(two_tables, generic, no_cluster, cluster_v1, variant, table, demig_ring, wide, wide_scalar,
-                           cluster2, wide_bulk)
+                           cluster2, wide_bulk, line_packing)
         h = ctypes.c_void_p()
         check(lib().img2d_plan_create(ctypes.byref(h), ns, nextrap, nz, nx, nf, nt, M, nk, ptr(x0), ptr(wn), flags))
         self._h = h
@@ -208,6 +210,7 @@ class Plan:
 N_CLUSTER2_VARIANTS = 12
 CANDIDATES = [("default", {})] + [("cluster2/v%d" % v, {"variant": v}) for v in range(1, N_CLUSTER2_VARIANTS + 1)] + \
              [("wide/ffma2", {"wide": True}), ("wide/ffma", {"wide_scalar": True}), ("wide/bulk", {"wide_bulk": True}),
+              ("wide/lines", {"wide": True, "line_packing": True}),
               ("cluster2", {"cluster2": True}),
               ("cluster1", {"cluster_v1": True}), ("single-cta", {"no_cluster": True})]
 
@@ -235,7 +238,7 @@ def autotune(ns, nextrap, nz, nx, nf, nt, M, nk, dk, omega, velocity, table, wav
         except LibraryError:
             continue
         d = plan.describe()
-        key = (d["kernel"], d["variant"], d["cluster"], d["G"], d["block"])
+        key = (d["kernel"], d["variant"], d["cluster"], d["G"], d["block"], d.get("packing"))
         if key in seen:
             plan.close()
             continue

@@ -47,6 +47,10 @@ typedef struct {
 /* the wide cluster kernel (packed FMAs) with its operator-pair ring filled by 1-D bulk copies
  * (cp.async.bulk, completing on per-warp transaction barriers) instead of 16-byte cp.async */
 #define IMG2D_FLAG_WIDE_BULK (1 << 18)
+/* wide cluster kernel: keep the line packing of the other kernels (shots chained into lane-slot
+ * lines across the model, lines grouped by extent) instead of the window-first packing, which the
+ * plan otherwise uses where its modelled cost is lower */
+#define IMG2D_FLAG_LINE_PACKING (1 << 19)
 /* Default kernel choice: the wide cluster kernel where the 16-slot kernel's clusters would leave
  * SMs idle (or fewer than 12 lane slots), else the 16-slot cluster kernel; the single-CTA kernels
  * for fewer than 6 lane slots, operators shorter than 7 taps or windows beyond 16 CTAs. */
