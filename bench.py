@@ -40,7 +40,8 @@ UNIT = "pts/s"
 # dram = (dram__bytes_read.sum + dram__bytes_write.sum) / points, l2 = lts__t_sectors.sum * 32 / points.
 # Keyed by (kernel, variant) of describe(); the bench scales them by the points of its launch.
 TRAFFIC_PER_POINT = {
-    ("migrate_wide", 3): {"dram": 2.41, "l2": 83.1, "capture": "migrate_wide_kernel<1, 1>, nz=60 nf=64"},
+    ("migrate_wide", 3): {"dram": 2.38, "l2": 82.4,
+                          "capture": "migrate_wide_kernel<1, 1, 0>, window packing, nz=60 nf=64"},
     ("migrate_cluster2", 11): {"dram": 0.980, "l2": 45.8, "capture": "migrate_cluster2_kernel ring variant, nz=60 nf=64"},
 }
 

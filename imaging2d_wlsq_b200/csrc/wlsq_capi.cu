@@ -411,6 +411,7 @@ struct img2d_plan {
     bool launched = false;  // a migration kernel has been queued (its status word is initialised)
     const char *packing = "lines";  // how shots were packed into the wide kernel's items
     double pack_cost = 0.0;         // wide kernel: modelled cost of all items of one frequency, in CTA units
+    double computed_per_useful = 0.0;  // computed (slot, position) pairs per aperture sample
     ~img2d_plan()
     {
         if (ev0) cudaEventDestroy(ev0);
@@ -911,6 +912,21 @@ static int build_plan(img2d_plan *p, int ns, int nextrap, int nz, int nx, int nf
     for (int g : gorder)
         for (int j = 0; j < nf; ++j) items.push_back(make_int2(g, j));
     p->n_items = (int)items.size();
+    {
+        // (slot, position) pairs the kernel computes per depth step and frequency, per useful one
+        double computed = 0.0, useful = 0.0;
+        for (int s = 0; s < ns; ++s) useful += p->w[s];
+        const int K = std::max(1, p->cluster);
+        for (const GroupDesc &g : groups) {
+            if (!strcmp(p->kname, "migrate_wide"))
+                computed += (double)K * std::min(WideShape::PC, (g.W + K * 256 - 1) / (K * 256) * 256) * p->G;
+            else if (!strcmp(p->kname, "migrate_cluster2"))
+                computed += (double)K * p->block * p->G;
+            else
+                computed += (double)g.W * p->G;
+        }
+        p->computed_per_useful = computed / useful;
+    }
     IMG2D_CUDA(cudaFuncSetAttribute(p->fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->smem));
     if (p->cluster) {
         cudaLaunchConfig_t cfg{};
@@ -1559,10 +1575,11 @@ int img2d_plan_describe(const img2d_plan *p, char *buf, int buflen)
     snprintf(buf, buflen,
              "{\"kernel\": \"%s\", \"cluster\": %d, \"G\": %d, \"X\": %d, \"L\": %d, \"grid\": %d, \"block\": %d, "
              "\"smem\": %zu, \"items\": %d, \"slots\": %d, \"max_union_width\": %d, \"mode\": %d, \"variant\": %d, "
-             "\"table\": \"%s\", \"packing\": \"%s\", \"cost_units\": %.3f}",
+             "\"table\": \"%s\", \"packing\": \"%s\", \"cost_units\": %.3f, \"computed_per_useful\": %.4f}",
              p->kname, p->cluster, p->G, p->fixed ? kX : 4, p->L, p->grid, p->block, p->smem,
              p->n_items, p->n_slots, p->max_w, p->mode, p->variant,
-             p->tab16 == 2 ? "bf16" : (p->tab16 == 1 ? "fp16" : "fp32"), p->packing, p->pack_cost);
+             p->tab16 == 2 ? "bf16" : (p->tab16 == 1 ? "fp16" : "fp32"), p->packing, p->pack_cost,
+             p->computed_per_useful);
     return IMG2D_OK;
 }
 
