@@ -560,15 +560,27 @@ static double wide_item_cost(int W, int K)
     return (double)K * NC / WideShape::PC / eff;
 }
 
-// Up to G lines of shots inside [u0, u1) from `pool` (shots sorted by aperture end): each line is
-// the heaviest chain of shots (total aperture width) separated by >= M, taken in turn (weighted
-// interval scheduling, repeated).  Returns the aperture width covered; the lines when asked.
-static long long window_lines(const img2d_plan *p, const std::vector<int> &pool, int u0, int u1, int G,
+// The shots of `pool` (sorted by aperture end) that lie inside [u0, u1), in that order; returns
+// their total aperture width.
+static long long window_shots(const img2d_plan *p, const std::vector<int> &pool, int u0, int u1,
+                              std::vector<int> &cand)
+{
+    cand.clear();
+    long long sum = 0;
+    for (int s : pool)
+        if (p->x0[s] >= u0 && p->x0[s] + p->w[s] <= u1) {
+            cand.push_back(s);
+            sum += p->w[s];
+        }
+    return sum;
+}
+
+// Up to G lines from the shots `cand` (sorted by aperture end): each line is the heaviest chain of
+// shots (total aperture width) separated by >= M, taken in turn (weighted interval scheduling,
+// repeated).  Returns the aperture width covered; the lines when asked.
+static long long window_lines(const img2d_plan *p, std::vector<int> cand, int G,
                               std::vector<std::vector<int>> *lines_out)
 {
-    std::vector<int> cand;
-    for (int s : pool)
-        if (p->x0[s] >= u0 && p->x0[s] + p->w[s] <= u1) cand.push_back(s);
     long long covered = 0;
     std::vector<long long> best, ends;
     std::vector<int> prev;
@@ -618,9 +630,9 @@ static long long window_lines(const img2d_plan *p, const std::vector<int> &pool,
 }
 
 // Window-first packing for the wide kernel: repeatedly take the window (a start on a 32-position
-// grid and a width of K x 256 x m positions, m = 1..4, the widths at which an item's cost steps)
-// whose G best lines of the remaining shots cover the most aperture per unit of cost, until every
-// shot is placed.  Narrow windows become narrow items, which the kernel runs with fewer busy warps
+// grid or at an end of one of the 8 widest remaining shots, and a width of K x 256 x m positions,
+// m = 1..4, the widths at which an item's cost steps) whose G best lines of the remaining shots
+// cover the most aperture per unit of cost, until every shot is placed.  Narrow windows become narrow items, which the kernel runs with fewer busy warps
 // instead of computing positions outside every aperture.  Returns the total cost in CTA units.
 static double pack_groups_windows(const img2d_plan *p, int G, int K, std::vector<GroupDesc> &groups,
                                   std::vector<int4> &segs, std::vector<int16_t> &owner)
@@ -635,27 +647,43 @@ static double pack_groups_windows(const img2d_plan *p, int G, int K, std::vector
     const int nx = p->nx;
     const int step = std::max(32, (nx / 64 + 31) / 32 * 32);
     double total = 0.0;
+    std::vector<int> starts, cand, prev;
     while (!pool.empty()) {
         double best_ratio = -1.0;
         int best_u0 = 0, best_w = 0;
+        // the 8 widest remaining shots also get windows aligned to either of their ends, so that a
+        // shot nearly as wide as a window still has one that holds it
+        std::vector<int> widest(pool);
+        std::stable_sort(widest.begin(), widest.end(), [&](int a, int b) { return p->w[a] > p->w[b]; });
+        widest.resize(std::min<size_t>(8, widest.size()));
         for (int m = 1; m <= 4; ++m) {
             const int W = std::min(nx, K * 256 * m);
             const double c = wide_item_cost(W, K);
-            for (int u = 0;; u += step) {
-                const int u0 = std::min(u, nx - W);
-                const long long cov = window_lines(p, pool, u0, u0 + W, G, nullptr);
+            starts.clear();
+            for (int u = 0; u <= std::max(nx - W, 0) + step - 1; u += step) starts.push_back(u);
+            for (int s : widest) starts.push_back(p->x0[s]);
+            for (int s : widest) starts.push_back(p->x0[s] + p->w[s] - W);
+            prev.clear();
+            for (int u : starts) {
+                const int u0 = std::max(0, std::min(u, nx - W));
+                // the total width of the shots inside bounds what G lines can cover; a window with
+                // the same shots as the previous one of this width covers the same
+                const long long bound = window_shots(p, pool, u0, u0 + W, cand);
+                if (bound == 0 || bound / c <= best_ratio || cand == prev) continue;
+                prev = cand;
+                const long long cov = window_lines(p, cand, G, nullptr);
                 if (cov > 0 && cov / c > best_ratio) {
                     best_ratio = cov / c;
                     best_u0 = u0;
                     best_w = W;
                 }
-                if (u0 >= nx - W) break;
             }
             if (W >= nx) break;
         }
         if (best_ratio <= 0.0) return -1.0;  // a shot wider than every window (not reached: K covers it)
         std::vector<std::vector<int>> lines;
-        window_lines(p, pool, best_u0, best_u0 + best_w, G, &lines);
+        window_shots(p, pool, best_u0, best_u0 + best_w, cand);
+        window_lines(p, cand, G, &lines);
         emit_group(p, lines, groups, segs, owner);
         total += wide_item_cost(groups.back().W, K);
         std::vector<char> placed(p->ns, 0);
@@ -810,21 +838,27 @@ static int build_plan(img2d_plan *p, int ns, int nextrap, int nz, int nx, int nf
         p->pack_cost = 0.0;
         for (const GroupDesc &g : groups) p->pack_cost += wide_item_cost(g.W, K);
         if (!(flags & IMG2D_FLAG_LINE_PACKING)) {
-            // window-first packing where it costs less, on clusters just wide enough for the widest shot
+            // window-first packing where it costs at least 1% less, on clusters just wide enough for
+            // the widest shot or one CTA wider (wider windows chain more shots per lane slot);
+            // cluster sizes beyond the portable 8 only where the line packing needs them anyway
             const int Kw = (*std::max_element(p->w.begin(), p->w.end()) + WideShape::PC - 1) / WideShape::PC;
-            std::vector<GroupDesc> g2;
-            std::vector<int4> s2;
-            std::vector<int16_t> o2;
-            const double cost2 = pack_groups_windows(p, WideShape::G, Kw, g2, s2, o2);
-            if (cost2 > 0.0 && cost2 < p->pack_cost * 0.99) {
-                groups.swap(g2);
-                segs.swap(s2);
-                owner.swap(o2);
-                K = Kw;
-                widest = 0;
-                for (const GroupDesc &g : groups) widest = std::max(widest, g.W);
-                p->packing = "windows";
-                p->pack_cost = cost2;
+            const int Kline = K;
+            for (int Kc = Kw; Kc <= Kw + 1; ++Kc) {
+                if (Kc > 8 && Kc != Kline) continue;
+                std::vector<GroupDesc> g2;
+                std::vector<int4> s2;
+                std::vector<int16_t> o2;
+                const double cost2 = pack_groups_windows(p, WideShape::G, Kc, g2, s2, o2);
+                if (cost2 > 0.0 && cost2 < p->pack_cost * 0.99) {
+                    groups.swap(g2);
+                    segs.swap(s2);
+                    owner.swap(o2);
+                    K = Kc;
+                    widest = 0;
+                    for (const GroupDesc &g : groups) widest = std::max(widest, g.W);
+                    p->packing = "windows";
+                    p->pack_cost = cost2;
+                }
             }
         }
         if (!(K <= 8 || (K <= kMaxCluster && clusters_that_fit((const void *)wf, K, WideShape::NW * 32, smemw) > 0)))
