@@ -418,6 +418,7 @@ struct img2d_plan {
         if (ev1) cudaEventDestroy(ev1);
     }
     int n_slots = 0;
+    std::vector<int> group_order;  // migration groups, widest first (the order of the item queue)
     int cluster = 0;  // CTAs per cluster of the cluster kernel, 0 = single-CTA kernels
     int block = 256;                  // threads per CTA of the chosen kernel
     int variant = -1;                 // index into the cluster2 variant table
@@ -946,6 +947,7 @@ static int build_plan(img2d_plan *p, int ns, int nextrap, int nz, int nx, int nf
     for (int g : gorder)
         for (int j = 0; j < nf; ++j) items.push_back(make_int2(g, j));
     p->n_items = (int)items.size();
+    p->group_order = gorder;
     {
         // (slot, position) pairs the kernel computes per depth step and frequency, per useful one
         double computed = 0.0, useful = 0.0;
@@ -1071,6 +1073,30 @@ static int read_status(img2d_plan *p, cudaStream_t st)
     return IMG2D_OK;
 }
 
+// The plan's persistent migration kernel on `grid` CTAs (whole clusters) of stream st.
+static int launch_kernel(img2d_plan *p, const MigrateArgs &a, int grid, cudaStream_t st)
+{
+    if (p->cluster) {
+        cudaLaunchConfig_t cfg{};
+        cudaLaunchAttribute attr{};
+        attr.id = cudaLaunchAttributeClusterDimension;
+        attr.val.clusterDim.x = p->cluster;
+        attr.val.clusterDim.y = 1;
+        attr.val.clusterDim.z = 1;
+        cfg.gridDim = dim3(grid, 1, 1);
+        cfg.blockDim = dim3(p->block, 1, 1);
+        cfg.dynamicSmemBytes = p->smem;
+        cfg.stream = st;
+        cfg.attrs = &attr;
+        cfg.numAttrs = 1;
+        IMG2D_CUDA(cudaLaunchKernelEx(&cfg, p->fn, a));
+    } else {
+        p->fn<<<grid, 256, p->smem, st>>>(a);
+    }
+    IMG2D_CUDA(cudaGetLastError());
+    return IMG2D_OK;
+}
+
 // Launch the persistent kernel and (optionally) reduce the stacked image.
 static int launch(img2d_plan *p, MigrateArgs a, float *d_image, float *d_image_shots,
                   long long img_sstride, cudaStream_t st)
@@ -1096,24 +1122,8 @@ static int launch(img2d_plan *p, MigrateArgs a, float *d_image, float *d_image_s
         IMG2D_CUDA(cudaEventCreate(&p->ev1));
     }
     if (p->timing) IMG2D_CUDA(cudaEventRecord(p->ev0, st));
-    if (p->cluster) {
-        cudaLaunchConfig_t cfg{};
-        cudaLaunchAttribute attr{};
-        attr.id = cudaLaunchAttributeClusterDimension;
-        attr.val.clusterDim.x = p->cluster;
-        attr.val.clusterDim.y = 1;
-        attr.val.clusterDim.z = 1;
-        cfg.gridDim = dim3(p->grid, 1, 1);
-        cfg.blockDim = dim3(p->block, 1, 1);
-        cfg.dynamicSmemBytes = p->smem;
-        cfg.stream = st;
-        cfg.attrs = &attr;
-        cfg.numAttrs = 1;
-        IMG2D_CUDA(cudaLaunchKernelEx(&cfg, p->fn, a));
-    } else {
-        p->fn<<<p->grid, 256, p->smem, st>>>(a);
-    }
-    IMG2D_CUDA(cudaGetLastError());
+    int rc;
+    if ((rc = launch_kernel(p, a, p->grid, st))) return rc;
     if (p->timing) {
         IMG2D_CUDA(cudaEventRecord(p->ev1, st));
         p->ev_recorded = true;
@@ -1368,7 +1378,124 @@ static int run_dense(int ns, int nextrap, int nz, int nx, int nf, int nt, int M,
 // (and freed) while it is the current device.
 struct HostEntryBuffers {
     DevBuf omega, vel, tabF, tabB, wave, shot, image, image_shots;
+    // frequency-chunked path: items per chunk, two sets of per-CTA image partials, the two queue
+    // counters and two status words, its streams (copies in, copies out, two for the kernels)
+    DevBuf chunk_items, pipe_partial, pipe_comp, pipe_counter;
+    const img2d_plan *chunk_plan = nullptr;  // the plan and chunk count chunk_items was built for
+    int chunks = 0;
+    std::vector<int> chunk_first;            // first item of each chunk, chunks + 1 entries
+    cudaStream_t st[4] = {nullptr, nullptr, nullptr, nullptr};
+    std::vector<cudaEvent_t> ev;
+    ~HostEntryBuffers()
+    {
+        for (cudaEvent_t e : ev) cudaEventDestroy(e);
+        for (cudaStream_t x : st)
+            if (x) cudaStreamDestroy(x);
+    }
 };
+
+// img2d_migrate_compact in C frequency chunks.  Each chunk's spectra go to the device, its items
+// run as one persistent launch and its final wavefields come back, on separate streams, so the
+// copies of one chunk overlap the kernels of the others.  The launches alternate between two
+// streams, each with its own work-queue counter and its own set of per-CTA image partials: a
+// launch's clusters start on the SMs that the previous launch's last items leave free, and the two
+// partial sets are summed once at the end.  Each launch is issued before the wavefields of the
+// previous chunk are copied back, so the GPU has queued work while a pageable copy holds the host.
+// The kernels and the per-item arithmetic are those of a single launch.
+static int migrate_chunked(img2d_plan *p, HostEntryBuffers &hb, int C, img2d_c64 *wave_fs, img2d_c64 *shot_fs,
+                           cpx *dW, cpx *dS, float *dI)
+{
+    int rc;
+    const int nf = p->nf;
+    const size_t plane = (size_t)p->nextrap * p->nx;
+    auto fbegin = [&](int c) { return (int)((long long)c * nf / C); };
+    if (hb.chunk_plan != p || hb.chunks != C) {
+        // within a chunk, widest groups first (the short items end the launch)
+        std::vector<int2> items;
+        hb.chunk_first.assign(1, 0);
+        for (int c = 0; c < C; ++c) {
+            for (int g : p->group_order)
+                for (int j = fbegin(c); j < fbegin(c + 1); ++j) items.push_back(make_int2(g, j));
+            hb.chunk_first.push_back((int)items.size());
+        }
+        if ((rc = hb.chunk_items.ensure(items.size() * sizeof(int2)))) return rc;
+        IMG2D_CUDA(cudaMemcpy(hb.chunk_items.p, items.data(), items.size() * sizeof(int2), cudaMemcpyHostToDevice));
+        hb.chunk_plan = p;
+        hb.chunks = C;
+    }
+    const size_t set_bytes = (size_t)p->grid * plane * sizeof(float);
+    if ((rc = hb.pipe_partial.ensure(2 * set_bytes))) return rc;
+    if ((rc = hb.pipe_comp.ensure(2 * set_bytes))) return rc;
+    if ((rc = hb.pipe_counter.ensure(4 * sizeof(int)))) return rc;
+    for (cudaStream_t &x : hb.st)
+        if (!x) IMG2D_CUDA(cudaStreamCreateWithFlags(&x, cudaStreamNonBlocking));
+    while ((int)hb.ev.size() < 2 * C + 1) {
+        cudaEvent_t e;
+        IMG2D_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        hb.ev.push_back(e);
+    }
+    cudaStream_t sin = hb.st[0], sout = hb.st[1], sk[2] = {hb.st[2], hb.st[3]};
+    int *cnt = hb.pipe_counter.as<int>();
+    float *part = hb.pipe_partial.as<float>(), *comp = hb.pipe_comp.as<float>();
+    // zeroed partial sets, counters and status words before the first launch of either stream
+    IMG2D_CUDA(cudaMemsetAsync(part, 0, 2 * set_bytes, sk[0]));
+    IMG2D_CUDA(cudaMemsetAsync(comp, 0, 2 * set_bytes, sk[0]));
+    IMG2D_CUDA(cudaMemsetAsync(cnt, 0, 4 * sizeof(int), sk[0]));
+    IMG2D_CUDA(cudaEventRecord(hb.ev[2 * C], sk[0]));
+    IMG2D_CUDA(cudaStreamWaitEvent(sk[1], hb.ev[2 * C], 0));
+    auto copy_rows = [&](int c, bool in) -> int {
+        const int f0 = fbegin(c), f1 = fbegin(c + 1);
+        for (int s = 0; s < p->ns; ++s) {
+            const long long off = p->off[s] + (long long)f0 * p->w[s];
+            const size_t bytes = (size_t)(f1 - f0) * p->w[s] * sizeof(cpx);
+            if (in) {
+                IMG2D_CUDA(cudaMemcpyAsync(dW + off, wave_fs + off, bytes, cudaMemcpyHostToDevice, sin));
+                IMG2D_CUDA(cudaMemcpyAsync(dS + off, shot_fs + off, bytes, cudaMemcpyHostToDevice, sin));
+            } else {
+                IMG2D_CUDA(cudaMemcpyAsync(wave_fs + off, dW + off, bytes, cudaMemcpyDeviceToHost, sout));
+                IMG2D_CUDA(cudaMemcpyAsync(shot_fs + off, dS + off, bytes, cudaMemcpyDeviceToHost, sout));
+            }
+        }
+        return IMG2D_OK;
+    };
+    const int K = std::max(1, p->cluster);
+    for (int c = 0; c < C; ++c) {
+        if ((rc = copy_rows(c, true))) return rc;
+        IMG2D_CUDA(cudaEventRecord(hb.ev[2 * c], sin));
+        cudaStream_t st = sk[c & 1];
+        IMG2D_CUDA(cudaStreamWaitEvent(st, hb.ev[2 * c], 0));
+        if (c >= 2) IMG2D_CUDA(cudaMemsetAsync(cnt + (c & 1), 0, sizeof(int), st));  // after launch c - 2
+        MigrateArgs a = base_args(p, dW, dS);
+        const int n = hb.chunk_first[c + 1] - hb.chunk_first[c];
+        a.items = hb.chunk_items.as<int2>() + hb.chunk_first[c];
+        a.n_items = n;
+        a.counter = cnt + (c & 1);
+        a.status = cnt + 2 + (c & 1);
+        a.partial = dI ? part + (size_t)(c & 1) * p->grid * plane : nullptr;
+        a.comp = dI ? comp + (size_t)(c & 1) * p->grid * plane : nullptr;
+        if ((rc = launch_kernel(p, a, std::min(n, p->grid / K) * K, st))) return rc;
+        IMG2D_CUDA(cudaEventRecord(hb.ev[2 * c + 1], st));
+        if (c >= 1) {
+            IMG2D_CUDA(cudaStreamWaitEvent(sout, hb.ev[2 * c - 1], 0));
+            if ((rc = copy_rows(c - 1, false))) return rc;
+        }
+    }
+    IMG2D_CUDA(cudaStreamWaitEvent(sout, hb.ev[2 * C - 1], 0));
+    if ((rc = copy_rows(C - 1, false))) return rc;
+    if (dI) {
+        IMG2D_CUDA(cudaStreamWaitEvent(sk[0], hb.ev[2 * C - 1], 0));
+        if (C >= 2) IMG2D_CUDA(cudaStreamWaitEvent(sk[0], hb.ev[2 * C - 3], 0));
+        const int blocks = (int)std::min<size_t>((plane + 255) / 256, 148 * 8);
+        reduce_partials_kernel<<<blocks, 256, 0, sk[0]>>>(part, comp, 2 * p->grid, (long long)plane, dI);
+        IMG2D_CUDA(cudaGetLastError());
+    }
+    for (cudaStream_t x : hb.st) IMG2D_CUDA(cudaStreamSynchronize(x));
+    int status[2] = {0, 0};
+    IMG2D_CUDA(cudaMemcpy(status, cnt + 2, sizeof(status), cudaMemcpyDeviceToHost));
+    if (status[0] || status[1])
+        return fail(IMG2D_ECUDA, "a bounded wait in the migration kernel gave up: the results of that call are not valid");
+    return IMG2D_OK;
+}
 struct HostCache {
     img2d_plan *plan = nullptr;
     std::vector<int> key;
@@ -1952,6 +2079,15 @@ int img2d_migrate_compact(int ns, int nextrap, int nz, int nx, int nf, int nt, i
     IMG2D_CUDA(cudaMemcpy(dV, velocity, (size_t)nextrap * nx * sizeof(double), cudaMemcpyHostToDevice));
     IMG2D_CUDA(cudaMemcpy(dTF, tab_forw, nk * L * sizeof(cpx), cudaMemcpyHostToDevice));
     if (dTB) IMG2D_CUDA(cudaMemcpy(dTB, tab_back, nk * L * sizeof(cpx), cudaMemcpyHostToDevice));
+    // large wavefields: frequency chunks whose copies overlap the other chunks' kernels
+    const int chunks = std::min(8, nf);
+    if (!image_shots && chunks >= 2 && p->wave_elems * sizeof(cpx) >= ((size_t)64 << 20)) {
+        if ((rc = set_model(p, dO, dV, dk, dTF, dTB, 0))) return rc;
+        IMG2D_CUDA(cudaDeviceSynchronize());
+        if ((rc = migrate_chunked(p, hb, chunks, wave_fs, shot_fs, dW, dS, dI))) return rc;
+        if (image) IMG2D_CUDA(cudaMemcpy(image, dI, (size_t)nextrap * nx * sizeof(float), cudaMemcpyDeviceToHost));
+        return IMG2D_OK;
+    }
     IMG2D_CUDA(cudaMemcpy(dW, wave_fs, p->wave_elems * sizeof(cpx), cudaMemcpyHostToDevice));
     IMG2D_CUDA(cudaMemcpy(dS, shot_fs, p->wave_elems * sizeof(cpx), cudaMemcpyHostToDevice));
     if ((rc = set_model(p, dO, dV, dk, dTF, dTB, 0))) return rc;

@@ -115,7 +115,11 @@ int img2d_migrate_compact(int ns, int nextrap, int nz, int nx, int nf, int nt, i
 /* img2d_migrate_compact keeps, per device, its plan (for the last geometry on that device) and its
  * device buffers (grown to the largest sizes seen) between calls, so repeated calls allocate
  * nothing.  img2d_release_host_cache frees them on every device; img2d_host_cache_device_count
- * is the number of devices that hold such a cache. */
+ * is the number of devices that hold such a cache.
+ * With 64 MiB of wavefields or more (and no per-shot images) a call runs in 8 frequency chunks: the
+ * host copies of each chunk overlap the kernels of the others (pinned host memory overlaps fully),
+ * on streams of its own, with a second set of per-CTA image partials.  It returns when everything
+ * is back in host memory, like a call in one piece. */
 void img2d_release_host_cache(void);
 int img2d_host_cache_device_count(void);
 
