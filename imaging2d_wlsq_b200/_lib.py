@@ -99,6 +99,9 @@ def load():
     lib.img2d_plan_kernel_ms.argtypes = [c_void_p, POINTER(ctypes.c_float)]
     lib.img2d_plan_status.restype = c_int
     lib.img2d_plan_status.argtypes = [c_void_p, c_void_p]
+    lib.img2d_pack_shots.restype = c_int
+    lib.img2d_pack_shots.argtypes = [c_int, c_int, c_int, c_void_p, c_void_p, c_int, c_int, c_void_p, c_void_p,
+                                     c_void_p, c_void_p, POINTER(c_int), POINTER(c_double)]
     lib.img2d_measure_fp32_peak.restype = c_int
     lib.img2d_measure_fp32_peak.argtypes = [POINTER(c_double)]
     lib.img2d_ricker_sources.restype = c_int

@@ -698,6 +698,46 @@ static double pack_groups_windows(const img2d_plan *p, int G, int K, std::vector
     return total;
 }
 
+// Pack shots into lane slots: shots sorted by aperture start go to the slot whose last shot ends
+// furthest to the left while still leaving >= M zero samples before this one (interval colouring,
+// best fit); full-aperture shots get a slot each.  Slots are then ordered by extent.  Needs x0, w
+// and M of the plan.
+static void colour_slots(img2d_plan *p)
+{
+    const int ns = (int)p->x0.size(), M = p->M;
+    std::vector<int> order(ns);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+        if (p->x0[a] != p->x0[b]) return p->x0[a] < p->x0[b];
+        return p->w[a] < p->w[b];
+    });
+    std::vector<std::vector<int>> slots;
+    std::vector<int> slot_end;
+    for (int s : order) {
+        int best = -1;
+        for (size_t i = 0; i < slots.size(); ++i)
+            if (slot_end[i] + M <= p->x0[s] && (best < 0 || slot_end[i] > slot_end[best])) best = (int)i;
+        if (best < 0) {
+            slots.push_back({s});
+            slot_end.push_back(p->x0[s] + p->w[s]);
+        } else {
+            slots[best].push_back(s);
+            slot_end[best] = p->x0[s] + p->w[s];
+        }
+    }
+    std::vector<int> sorder(slots.size());
+    std::iota(sorder.begin(), sorder.end(), 0);
+    auto ext0 = [&](int i) { return p->x0[slots[i].front()]; };
+    std::stable_sort(sorder.begin(), sorder.end(), [&](int a, int b) {
+        if (ext0(a) != ext0(b)) return ext0(a) < ext0(b);
+        return slot_end[a] < slot_end[b];
+    });
+    p->n_slots = (int)slots.size();
+    p->slots = slots;
+    p->slot_order = sorder;
+    p->slot_end = slot_end;
+}
+
 static int build_plan(img2d_plan *p, int ns, int nextrap, int nz, int nx, int nf, int nt, int M,
                       int nk, const int *shot_x0, const int *shot_nx, int flags, int mode)
 {
@@ -732,40 +772,7 @@ static int build_plan(img2d_plan *p, int ns, int nextrap, int nz, int nx, int nf
     IMG2D_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
     const int static_reserve = 1024;
 
-    // Pack shots into lane slots: shots sorted by aperture start go to the slot whose last shot
-    // ends furthest to the left while still leaving >= M zero samples before this one (interval
-    // colouring, best fit); full-aperture shots get a slot each.
-    std::vector<int> order(ns);
-    std::iota(order.begin(), order.end(), 0);
-    std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
-        if (p->x0[a] != p->x0[b]) return p->x0[a] < p->x0[b];
-        return p->w[a] < p->w[b];
-    });
-    std::vector<std::vector<int>> slots;
-    std::vector<int> slot_end;
-    for (int s : order) {
-        int best = -1;
-        for (size_t i = 0; i < slots.size(); ++i)
-            if (slot_end[i] + M <= p->x0[s] && (best < 0 || slot_end[i] > slot_end[best])) best = (int)i;
-        if (best < 0) {
-            slots.push_back({s});
-            slot_end.push_back(p->x0[s] + p->w[s]);
-        } else {
-            slots[best].push_back(s);
-            slot_end[best] = p->x0[s] + p->w[s];
-        }
-    }
-    std::vector<int> sorder(slots.size());
-    std::iota(sorder.begin(), sorder.end(), 0);
-    auto ext0 = [&](int i) { return p->x0[slots[i].front()]; };
-    std::stable_sort(sorder.begin(), sorder.end(), [&](int a, int b) {
-        if (ext0(a) != ext0(b)) return ext0(a) < ext0(b);
-        return slot_end[a] < slot_end[b];
-    });
-    p->n_slots = (int)slots.size();
-    p->slots = slots;
-    p->slot_order = sorder;
-    p->slot_end = slot_end;
+    colour_slots(p);
 
     std::vector<GroupDesc> groups;
     std::vector<int4> segs;
@@ -1752,6 +1759,54 @@ int img2d_plan_kernel_ms(img2d_plan *p, float *ms)
     if (!p->ev_recorded) return fail(IMG2D_EINVAL, "no kernel launched on this plan yet");
     IMG2D_CUDA(cudaEventSynchronize(p->ev1));
     IMG2D_CUDA(cudaEventElapsedTime(ms, p->ev0, p->ev1));
+    return IMG2D_OK;
+}
+
+int img2d_pack_shots(int ns, int nx, int M, const int *shot_x0, const int *shot_nx, int windows, int K,
+                     int *group_of_shot, int *slot_of_shot, int *group_u0, int *group_w, int *n_groups,
+                     double *cost_units)
+{
+    if (ns <= 0 || nx <= 0 || M < 0 || !shot_x0 || !shot_nx || !group_of_shot || !slot_of_shot || !n_groups)
+        return fail(IMG2D_EINVAL, "img2d_pack_shots: invalid arguments");
+    if (ns > 32767) return fail(IMG2D_EINVAL, "at most 32767 shots");
+    img2d_plan pl;
+    pl.ns = ns;
+    pl.nx = nx;
+    pl.M = M;
+    pl.x0.assign(shot_x0, shot_x0 + ns);
+    pl.w.assign(shot_nx, shot_nx + ns);
+    int wmax = 0;
+    for (int s = 0; s < ns; ++s) {
+        if (pl.x0[s] < 0 || pl.w[s] <= 0 || pl.x0[s] + pl.w[s] > nx)
+            return fail(IMG2D_EINVAL, "shot " + std::to_string(s) + " aperture outside [0, nx)");
+        wmax = std::max(wmax, pl.w[s]);
+    }
+    const int Kmin = (wmax + WideShape::PC - 1) / WideShape::PC;
+    std::vector<GroupDesc> groups;
+    std::vector<int4> segs;
+    std::vector<int16_t> owner;
+    double cost = 0.0;
+    if (windows) {
+        if (K < Kmin) return fail(IMG2D_EINVAL, "K too small for the widest shot");
+        cost = pack_groups_windows(&pl, WideShape::G, K, groups, segs, owner);
+        if (cost < 0.0) return fail(IMG2D_EINVAL, "a shot fits no window");
+    } else {
+        colour_slots(&pl);
+        const int widest = pack_groups(&pl, WideShape::G, groups, segs, owner);
+        if (K <= 0) K = (widest + WideShape::PC - 1) / WideShape::PC;
+        if (K * WideShape::PC < widest) return fail(IMG2D_EINVAL, "K too small for the widest group");
+        for (const GroupDesc &g : groups) cost += wide_item_cost(g.W, K);
+    }
+    for (size_t g = 0; g < groups.size(); ++g) {
+        if (group_u0) group_u0[g] = groups[g].u0;
+        if (group_w) group_w[g] = groups[g].W;
+        for (int k = groups[g].seg_begin; k < groups[g].seg_begin + groups[g].nseg; ++k) {
+            group_of_shot[segs[k].x] = (int)g;
+            slot_of_shot[segs[k].x] = segs[k].y;
+        }
+    }
+    *n_groups = (int)groups.size();
+    if (cost_units) *cost_units = cost;
     return IMG2D_OK;
 }
 

@@ -76,6 +76,29 @@ def _wide_flags(wide, wide_scalar, wide_bulk=False):
     return _lib.FLAG_WIDE | (_lib.FLAG_WIDE_SCALAR if wide_scalar else 0) | (_lib.FLAG_WIDE_BULK if wide_bulk else 0)
 
 
+def pack_shots(shot_x0, shot_nx, nx, M, windows=True, K=None):
+    """The wide kernel's packing of shots into items of up to 8 lane slots, computed on the host
+    (no GPU): windows=True the window-first packing on clusters of K CTAs (default: just wide enough
+    for the widest shot), False the line packing.  Returns a dict with per-shot `group` and `slot`,
+    per-group `u0` and `width`, and the modelled `cost` of one frequency's items in CTA units."""
+    x0 = np.ascontiguousarray(shot_x0, dtype=np.int32)
+    wn = np.ascontiguousarray(shot_nx, dtype=np.int32)
+    ns = len(x0)
+    if K is None:
+        K = -(-int(wn.max()) // 1024) if windows else 0
+    group = np.empty(ns, np.int32)
+    slot = np.empty(ns, np.int32)
+    u0 = np.empty(ns, np.int32)
+    width = np.empty(ns, np.int32)
+    ng = ctypes.c_int()
+    cost = ctypes.c_double()
+    check(lib().img2d_pack_shots(ns, int(nx), int(M), ptr(x0), ptr(wn), int(bool(windows)), int(K), ptr(group),
+                                 ptr(slot), ptr(u0), ptr(width), ctypes.byref(ng), ctypes.byref(cost)))
+    n = ng.value
+    return {"group": group, "slot": slot, "u0": u0[:n].copy(), "width": width[:n].copy(), "cost": cost.value,
+            "K": int(K)}
+
+
 def fp32_peak_tflops():
     """Measured FP32 FMA throughput of the current GPU (TFLOP/s)."""
     v = ctypes.c_double()

@@ -164,6 +164,15 @@ int img2d_plan_kernel_ms(img2d_plan *plan, float *ms);
  * img2d_migrate_compact checks it by itself. */
 int img2d_plan_status(img2d_plan *plan, void *stream);
 
+/* Host only (no GPU needed): the wide kernel's packing of shots into items of up to 8 lane slots.
+ * windows = 0: the line packing (K <= 0: clusters just wide enough for its widest group);
+ * windows = 1: the window-first packing on clusters of K CTAs of 1024 positions.  Writes, per shot,
+ * its group and lane slot; per group (arrays of at least ns entries, may be NULL) its window start
+ * and width; the number of groups, and the modelled cost of one frequency's items in CTA units. */
+int img2d_pack_shots(int ns, int nx, int M, const int *shot_x0, const int *shot_nx, int windows, int K,
+                     int *group_of_shot, int *slot_of_shot, int *group_u0, int *group_w, int *n_groups,
+                     double *cost_units);
+
 /* FP32 FMA throughput of the current device in TFLOP/s, measured by a short kernel of independent
  * FMA chains (the denominator of the FP32 roofline; not part of the migration path). */
 int img2d_measure_fp32_peak(double *tflops);
