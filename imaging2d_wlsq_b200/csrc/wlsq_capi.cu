@@ -1,6 +1,7 @@
 // C ABI of the B200 extrapolation + imaging library: plans, kernel dispatch and the
 // reference-compatible entry points.  Declarations and contracts: include/imaging2d_wlsq_b200.h.
 #include <algorithm>
+#include <atomic>
 #include <map>
 #include <cstdio>
 #include <cstdlib>
@@ -409,6 +410,13 @@ struct img2d_plan {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     bool ev_recorded = false;
     bool launched = false;  // a migration kernel has been queued (its status word is initialised)
+    // identity of this plan for caches keyed on it (a new plan may reuse a freed plan's address)
+    const unsigned long long uid = next_uid();
+    static unsigned long long next_uid()
+    {
+        static std::atomic<unsigned long long> n{0};
+        return ++n;
+    }
     const char *packing = "lines";  // how shots were packed into the wide kernel's items
     double pack_cost = 0.0;         // wide kernel: modelled cost of all items of one frequency, in CTA units
     double computed_per_useful = 0.0;  // computed (slot, position) pairs per aperture sample
@@ -1388,7 +1396,7 @@ struct HostEntryBuffers {
     // frequency-chunked path: items per chunk, two sets of per-CTA image partials, the two queue
     // counters and two status words, its streams (copies in, copies out, two for the kernels)
     DevBuf chunk_items, pipe_partial, pipe_comp, pipe_counter;
-    const img2d_plan *chunk_plan = nullptr;  // the plan and chunk count chunk_items was built for
+    unsigned long long chunk_plan = 0;       // uid of the plan and chunk count chunk_items was built for
     int chunks = 0;
     std::vector<int> chunk_first;            // first item of each chunk, chunks + 1 entries
     cudaStream_t st[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -1416,7 +1424,7 @@ static int migrate_chunked(img2d_plan *p, HostEntryBuffers &hb, int C, img2d_c64
     const int nf = p->nf;
     const size_t plane = (size_t)p->nextrap * p->nx;
     auto fbegin = [&](int c) { return (int)((long long)c * nf / C); };
-    if (hb.chunk_plan != p || hb.chunks != C) {
+    if (hb.chunk_plan != p->uid || hb.chunks != C) {
         // within a chunk, widest groups first (the short items end the launch)
         std::vector<int2> items;
         hb.chunk_first.assign(1, 0);
@@ -1427,7 +1435,7 @@ static int migrate_chunked(img2d_plan *p, HostEntryBuffers &hb, int C, img2d_c64
         }
         if ((rc = hb.chunk_items.ensure(items.size() * sizeof(int2)))) return rc;
         IMG2D_CUDA(cudaMemcpy(hb.chunk_items.p, items.data(), items.size() * sizeof(int2), cudaMemcpyHostToDevice));
-        hb.chunk_plan = p;
+        hb.chunk_plan = p->uid;
         hb.chunks = C;
     }
     const size_t set_bytes = (size_t)p->grid * plane * sizeof(float);

@@ -54,3 +54,22 @@ def test_chunked_host_entry_matches_device_plan_and_oracle(pinned):
                                 w.table, wave2, shot2, shot_x0=w.shot_x0, shot_nx=w.shot_nx)
     np.testing.assert_array_equal(wave2, wave)
     assert rel_l2(img2, img) <= 1e-6
+
+
+def test_chunked_host_entry_after_a_geometry_change():
+    """A second geometry replaces the cached plan; the chunked call must rebuild its item lists for
+    the new plan's groups, even where the new plan reuses the old one's memory."""
+    from imaging2d_wlsq_b200 import sharding
+    w = synthetic.batched_uneven(nz=6, nf=40)
+    for idx in (np.arange(0, w.ns), np.arange(0, w.ns, 2), np.arange(1, w.ns, 2)):
+        sub = sharding.sub_workload(w, idx)
+        if sub.wave.nbytes < 64 << 20:
+            sub = sharding.sub_workload(synthetic.batched_uneven(nz=6, nf=80), idx)
+        assert sub.wave.nbytes >= 64 << 20
+        img_d, wave_d, _ = _device_plan_result(sub)
+        wave, shot = sub.wave.copy(), sub.shot.copy()
+        img, _ = migration.migrate(sub.ns, sub.nextrap, sub.nz, sub.nx, sub.nf, sub.nt, sub.M, sub.nk, sub.dk,
+                                   sub.omega, sub.velocity, sub.table, wave, shot, shot_x0=sub.shot_x0,
+                                   shot_nx=sub.shot_nx)
+        np.testing.assert_array_equal(wave, wave_d)
+        assert rel_l2(img, img_d) <= 1e-6
