@@ -1393,9 +1393,10 @@ static int run_dense(int ns, int nextrap, int nz, int nx, int nf, int nt, int M,
 // (and freed) while it is the current device.
 struct HostEntryBuffers {
     DevBuf omega, vel, tabF, tabB, wave, shot, image, image_shots;
-    // frequency-chunked path: items per chunk, two sets of per-CTA image partials, the two queue
-    // counters and two status words, its streams (copies in, copies out, two for the kernels)
-    DevBuf chunk_items, pipe_partial, pipe_comp, pipe_counter;
+    // frequency-chunked path: items per chunk, the two queue counters and two status words, its
+    // streams (copies in, copies out, two for the kernels); its two sets of per-CTA image partials
+    // are the plan's partial buffers, grown to twice the single-launch size
+    DevBuf chunk_items, pipe_counter;
     unsigned long long chunk_plan = 0;       // uid of the plan and chunk count chunk_items was built for
     int chunks = 0;
     std::vector<int> chunk_first;            // first item of each chunk, chunks + 1 entries
@@ -1439,8 +1440,8 @@ static int migrate_chunked(img2d_plan *p, HostEntryBuffers &hb, int C, img2d_c64
         hb.chunks = C;
     }
     const size_t set_bytes = (size_t)p->grid * plane * sizeof(float);
-    if ((rc = hb.pipe_partial.ensure(2 * set_bytes))) return rc;
-    if ((rc = hb.pipe_comp.ensure(2 * set_bytes))) return rc;
+    if ((rc = p->partial.ensure(2 * set_bytes))) return rc;
+    if ((rc = p->comp.ensure(2 * set_bytes))) return rc;
     if ((rc = hb.pipe_counter.ensure(4 * sizeof(int)))) return rc;
     for (cudaStream_t &x : hb.st)
         if (!x) IMG2D_CUDA(cudaStreamCreateWithFlags(&x, cudaStreamNonBlocking));
@@ -1451,7 +1452,7 @@ static int migrate_chunked(img2d_plan *p, HostEntryBuffers &hb, int C, img2d_c64
     }
     cudaStream_t sin = hb.st[0], sout = hb.st[1], sk[2] = {hb.st[2], hb.st[3]};
     int *cnt = hb.pipe_counter.as<int>();
-    float *part = hb.pipe_partial.as<float>(), *comp = hb.pipe_comp.as<float>();
+    float *part = p->partial.as<float>(), *comp = p->comp.as<float>();
     // zeroed partial sets, counters and status words before the first launch of either stream
     IMG2D_CUDA(cudaMemsetAsync(part, 0, 2 * set_bytes, sk[0]));
     IMG2D_CUDA(cudaMemsetAsync(comp, 0, 2 * set_bytes, sk[0]));
@@ -2147,7 +2148,12 @@ int img2d_migrate_compact(int ns, int nextrap, int nz, int nx, int nf, int nt, i
     if (!image_shots && chunks >= 2 && p->wave_elems * sizeof(cpx) >= ((size_t)64 << 20)) {
         if ((rc = set_model(p, dO, dV, dk, dTF, dTB, 0))) return rc;
         IMG2D_CUDA(cudaDeviceSynchronize());
-        if ((rc = migrate_chunked(p, hb, chunks, wave_fs, shot_fs, dW, dS, dI))) return rc;
+        if ((rc = migrate_chunked(p, hb, chunks, wave_fs, shot_fs, dW, dS, dI))) {
+            // leave no queued work behind on the error path
+            for (cudaStream_t x : hb.st)
+                if (x && cudaStreamSynchronize(x) != cudaSuccess) cudaGetLastError();
+            return rc;
+        }
         if (image) IMG2D_CUDA(cudaMemcpy(image, dI, (size_t)nextrap * nx * sizeof(float), cudaMemcpyDeviceToHost));
         return IMG2D_OK;
     }
