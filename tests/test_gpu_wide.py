@@ -152,7 +152,7 @@ def test_window_packing_matches_line_packing_and_oracle(case):
     the line packing: bit-identical wavefields (the per-point FMA sequence does not depend on the
     packing), images within 1e-6 of each other and 1e-5 of the FP64 oracle, and a lower modelled
     cost."""
-    # modelled costs (window against line packing): 3.27 against 3.43, and 5.14 against 6.00
+    # modelled costs (window against line packing): 3.28 against 3.45, and 5.15 against 6.00
     w = synthetic.batched_uneven(seed=4, scale=0.25, nz=40, nf=16) if case == "uneven" else _narrow_shots()
     d_win = migration.Plan.for_workload(w, wide=True).describe()
     d_lin = migration.Plan.for_workload(w, wide=True, line_packing=True).describe()

@@ -13,7 +13,7 @@ from imaging2d_wlsq_b200 import migration, synthetic
 
 def _item_cost(W, K):
     NC = min(1024, -(-W // (K * 256)) * 256)
-    eff = 1.0 if NC >= 1024 else (0.95 if NC >= 768 else (0.875 if NC >= 512 else 0.6))
+    eff = 1.0 if NC >= 1024 else (0.92 if NC >= 768 else (0.87 if NC >= 512 else 0.62))
     return K * NC / 1024 / eff
 
 
@@ -58,14 +58,14 @@ def test_packing_invariants(seed, ns, nx, lo, hi, windows):
 
 def test_window_packing_on_the_benchmark_survey():
     """256 shots of U[256, 2048] traces on 2048 positions (35 taps): the window-first packing models
-    36.6 CTA units per frequency against 38.3 for the line packing (measured 4.1% faster)."""
+    36.9 CTA units per frequency against 38.4 for the line packing (measured 4.1% faster)."""
     w = synthetic.batched_uneven(tables=False, nf=4)
     lines = migration.pack_shots(w.shot_x0, w.shot_nx, w.nx, w.M, windows=False)
     wins = migration.pack_shots(w.shot_x0, w.shot_nx, w.nx, w.M, windows=True)
     _check(w.shot_x0.astype(np.int64), w.shot_nx.astype(np.int64), w.nx, w.M, lines)
     _check(w.shot_x0.astype(np.int64), w.shot_nx.astype(np.int64), w.nx, w.M, wins)
     assert wins["cost"] < 0.97 * lines["cost"], (wins["cost"], lines["cost"])
-    assert abs(wins["cost"] - 36.617) < 0.01 and abs(lines["cost"] - 38.301) < 0.01
+    assert abs(wins["cost"] - 36.932) < 0.01 and abs(lines["cost"] - 38.410) < 0.01
 
 
 def test_pack_shots_rejects_bad_input():
