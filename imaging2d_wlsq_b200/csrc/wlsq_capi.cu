@@ -748,14 +748,21 @@ static void colour_slots(img2d_plan *p)
     p->slot_end = slot_end;
 }
 
+// Surveys with more shots keep the line packing: the window greedy would take seconds per plan.
+constexpr int kWindowPackingMaxShots = 2048;
+
 // The window-first packing with three weightings of 12-warp items in the greedy's choices (the
 // measured 0.92, then 0.95 and 1.0: a myopic greedy lands on different packings); keeps the one of
-// lowest measured-model cost.
+// lowest measured-model cost.  The greedy's time grows about as the square of the shot count
+// (0.4 s for 1024 shots on one host core), so above 512 shots only the measured weighting runs.
 static double pack_windows_best(const img2d_plan *p, int G, int K, std::vector<GroupDesc> &groups,
                                 std::vector<int4> &segs, std::vector<int16_t> &owner)
 {
     double best = -1.0;
-    for (double sel : {0.92, 0.95, 1.0}) {
+    const double sels[3] = {0.92, 0.95, 1.0};
+    const int nsel = p->ns > 512 ? 1 : 3;
+    for (int i = 0; i < nsel; ++i) {
+        const double sel = sels[i];
         std::vector<GroupDesc> g2;
         std::vector<int4> s2;
         std::vector<int16_t> o2;
@@ -877,7 +884,7 @@ static int build_plan(img2d_plan *p, int ns, int nextrap, int nz, int nx, int nf
         p->packing = "lines";
         p->pack_cost = 0.0;
         for (const GroupDesc &g : groups) p->pack_cost += wide_item_cost(g.W, K);
-        if (!(flags & IMG2D_FLAG_LINE_PACKING)) {
+        if (!(flags & IMG2D_FLAG_LINE_PACKING) && p->ns <= kWindowPackingMaxShots) {
             // window-first packing where it costs at least 1% less, on clusters just wide enough for
             // the widest shot or one CTA wider (wider windows chain more shots per lane slot);
             // cluster sizes beyond the portable 8 only where the line packing needs them anyway
