@@ -73,3 +73,38 @@ def test_chunked_host_entry_after_a_geometry_change():
                                    shot_nx=sub.shot_nx)
         np.testing.assert_array_equal(wave, wave_d)
         assert rel_l2(img, img_d) <= 1e-6
+
+
+def test_chunked_host_entry_with_more_rows_than_frequencies():
+    """Packed spectra of nt > nf rows per shot (the reference's layout: only the first nf rows are
+    extrapolated): the chunked call moves only those rows, leaves the others untouched, and gives
+    the result of the tight layout."""
+    w = synthetic.batched_uneven(nz=6, nf=40)
+    nt = w.nf + 3
+    img_ref, wave_ref, shot_ref = _device_plan_result(w)
+
+    def pad(a, fill):
+        out = []
+        for s in range(w.ns):
+            blk = w.block(a, s)
+            extra = np.full((nt - w.nf, blk.shape[1]), fill, dtype=np.complex64)
+            out.append(np.concatenate([blk, extra]).reshape(-1))
+        return np.concatenate(out)
+
+    wave = pad(w.wave, 7 + 7j)
+    shot = pad(w.shot, -3 + 1j)
+    assert wave.nbytes >= 64 << 20
+    img, _ = migration.migrate(w.ns, w.nextrap, w.nz, w.nx, w.nf, nt, w.M, w.nk, w.dk, w.omega, w.velocity,
+                               w.table, wave, shot, shot_x0=w.shot_x0, shot_nx=w.shot_nx)
+    off = 0
+    ref_off = 0
+    for s in range(w.ns):
+        n = int(w.shot_nx[s])
+        blk_w = wave[off:off + nt * n].reshape(nt, n)
+        blk_s = shot[off:off + nt * n].reshape(nt, n)
+        np.testing.assert_array_equal(blk_w[:w.nf].reshape(-1), wave_ref[ref_off:ref_off + w.nf * n])
+        np.testing.assert_array_equal(blk_s[:w.nf].reshape(-1), shot_ref[ref_off:ref_off + w.nf * n])
+        assert np.all(blk_w[w.nf:] == np.complex64(7 + 7j)) and np.all(blk_s[w.nf:] == np.complex64(-3 + 1j))
+        off += nt * n
+        ref_off += w.nf * n
+    assert rel_l2(img, img_ref) <= 1e-6
